@@ -1,0 +1,378 @@
+"""Benchmark: FFBF scan throughput on one B200 (or N independent replicas).
+
+Default workload ("scale"): 1,000,000 Zipf-word patterns of 32-64 bytes, LEN 32, filter geometry K 5, S 2,
+2^23 cache bits + 2^26 external bits (9 MiB, L2-resident); a 4 GiB text of the same letters with '\\n' every
+geometric(mean 100) bytes and 20,000 planted occurrences; all from one seed (synthetic data, see
+ffbf_b200/datagen.py).
+
+One step = one pass of the scan over the whole text: zero the feed-forward filter, then run the scan kernel
+(hash every window, probe the main filter, set feed-forward bits for hits, record hit windows and per-tile
+newline summaries). `value` is text GB/s with the text resident in HBM, timed with CUDA events on the
+library's stream; the 4 GiB input is larger than L2, so no flush is needed between steps. `e2e` is the same
+metric through the public C ABI from pinned host memory: ffbf_scan (H2D copy, scan, hit/line collection)
++ ffbf_prune + ffbf_verify, with every result copied back to the host.
+
+    python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload scale|plain|binary]
+
+With --impl reference the same workload is scanned by efficient/ffbf's own x86 binary (oracle/_ref, built
+from the reference sources) on all host cores: one process per core, each on its own line-aligned shard of
+the text, filter loaded from a __bloom_filter_ cache; throughput = shard bytes / the slowest process's
+`processFile time` (the reference's own timer).
+"""
+import argparse
+import json
+import os
+import shutil
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "scan GB/s & %HBM roofline at 1M patterns"
+UNIT = "GB/s"
+
+
+def parse():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
+    ap.add_argument("--workload", choices=["scale", "plain", "binary"], default="scale")
+    ap.add_argument("--text-bytes", type=int, default=0, help="override the workload's text size")
+    ap.add_argument("--seed", type=int, default=2024)
+    ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (default: min(steps, 5))")
+    ap.add_argument("--cpu-sample", type=int, default=1 << 30, help="bytes of text for the CPU baseline")
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    return ap.parse_args()
+
+
+def workload(args):
+    from ffbf_b200 import datagen as dg
+    fn = {"scale": dg.scale, "plain": dg.plain, "binary": dg.binary}[args.workload]
+    return fn(args.text_bytes) if args.text_bytes else fn()
+
+
+def describe(wl):
+    p = wl.params
+    return {"workload": f"{wl.name}: {wl.n_patterns} patterns ({wl.len_lo}-{wl.len_hi} B), LEN {p.len}, "
+                        f"{wl.text_bytes / 2**30:.3g} GiB text, {wl.n_plant} planted",
+            "geometry": {"len": p.len, "k": p.k, "s": p.s, "cache_bits": p.cache_bits, "ext_bits": p.ext_bits},
+            "text_bytes": wl.text_bytes, "n_patterns": wl.n_patterns,
+            "l2": "inputs larger than L2 (text > 126 MB), no flush"}
+
+
+# ---- clocks -------------------------------------------------------------------------------------------
+class ClockSampler:
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_id):
+        self.path = tempfile.mktemp(prefix="ffbf_clocks_", suffix=".csv")
+        self.proc = None
+        self.gpu_id = gpu_id
+
+    def start(self):
+        if not shutil.which("nvidia-smi"):
+            return
+        self.out = open(self.path, "w")
+        cmd = ["nvidia-smi", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits", "-lms", "100"]
+        if self.gpu_id is not None:
+            cmd += ["-i", str(self.gpu_id)]
+        self.proc = subprocess.Popen(cmd, stdout=self.out, stderr=subprocess.DEVNULL)
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": [], "samples": 0}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        self.out.close()
+        sm, mx, reasons, power = [], [], set(), []
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            f = [x.strip() for x in line.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+                power.append(float(f[3]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm), "power_w_max": max(power) if power else None}
+
+
+def gpu_id_for(dev):
+    import torch
+    try:
+        p = torch.cuda.get_device_properties(dev)
+        return f"{p.pci_domain_id:08x}:{p.pci_bus_id:02x}:{p.pci_device_id:02x}.0"
+    except Exception:
+        vis = os.environ.get("CUDA_VISIBLE_DEVICES")
+        return vis.split(",")[dev] if vis else dev
+
+
+def measured_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(p):
+        d = json.load(open(p))
+        return float(d["hbm_gbs"]), "measured"
+    return 6650.0, "fallback"
+
+
+# ---- the reference on the host cores ----------------------------------------------------------------
+def line_shards(text, n_shards, shard_bytes):
+    """Line-aligned [a, b) slices: shard i starts after the first '\\n' at or past i*shard_bytes."""
+    out = []
+    for i in range(n_shards):
+        a = i * shard_bytes
+        b = (i + 1) * shard_bytes
+        if b > text.size:
+            break
+        if a > 0:
+            nl = np.flatnonzero(text[a:a + 65536] == 10)
+            a = a + int(nl[0]) + 1 if nl.size else a
+        nl = np.flatnonzero(text[b:b + 65536] == 10)
+        b = b + int(nl[0]) + 1 if nl.size else b
+        out.append((a, min(b, text.size)))
+    return out
+
+
+def reference_binary(prm):
+    import oracle
+    return oracle.ref_binary(prm, build=os.path.exists(oracle.DEFAULT_REF_SRC))
+
+
+def prepare_reference_dirs(binary, pats, text, shards):
+    """One scratch dir per shard holding pats, the shard text and a __bloom_filter_pats cache built by the
+    reference itself (one run over an empty text)."""
+    base = tempfile.mkdtemp(prefix="ffbf_refbench_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
+    seed_dir = os.path.join(base, "seed")
+    os.makedirs(seed_dir)
+    with open(os.path.join(seed_dir, "pats"), "wb") as f:
+        f.write(pats.tobytes())
+    open(os.path.join(seed_dir, "empty"), "wb").close()
+    with open(os.path.join(seed_dir, "empty"), "rb") as fin:
+        subprocess.run([binary, "pats", "out"], stdin=fin, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
+                       cwd=seed_dir, check=True)
+    dirs = []
+    for i, (a, b) in enumerate(shards):
+        d = os.path.join(base, f"s{i}")
+        os.makedirs(d)
+        os.link(os.path.join(seed_dir, "pats"), os.path.join(d, "pats"))
+        shutil.copyfile(os.path.join(seed_dir, "__bloom_filter_pats"), os.path.join(d, "__bloom_filter_pats"))
+        text[a:b].tofile(os.path.join(d, "text"))
+        dirs.append((d, b - a))
+    return base, dirs
+
+
+def run_reference_step(binary, dirs):
+    procs = []
+    for d, _ in dirs:
+        fin = open(os.path.join(d, "text"), "rb")
+        p = subprocess.Popen([binary, "pats", "out"], stdin=fin, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
+                             cwd=d)
+        procs.append((p, fin))
+    times = []
+    for p, fin in procs:
+        _, err = p.communicate()
+        fin.close()
+        if p.returncode != 0:
+            raise RuntimeError(f"reference exited {p.returncode}: {err.decode(errors='replace')}")
+        t = [float(x.split(b":")[1]) for x in err.splitlines() if x.startswith(b"processFile time:")]
+        times.append(t[0])
+    return max(times)
+
+
+def cpu_baseline_single(wl, pats, text, sample_bytes):
+    """The reference binary on one core over a bounded, line-aligned prefix of the workload text."""
+    binary = reference_binary(wl.params)
+    if binary is None:
+        return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                "sample": "unavailable: reference binary for this geometry was not built"}
+    shards = line_shards(text, 1, min(sample_bytes, text.size - 65536))
+    base, dirs = prepare_reference_dirs(binary, pats, text, shards)
+    try:
+        t = run_reference_step(binary, dirs)
+    finally:
+        shutil.rmtree(base, ignore_errors=True)
+    nbytes = dirs[0][1]
+    return {"value": nbytes / t / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{nbytes / 2**20:.0f} MiB line-aligned prefix of the workload text, 1 process, filter "
+                      f"loaded from its __bloom_filter_ cache; processFile time {t:.3f} s"}
+
+
+def main_reference(args):
+    rank = int(os.environ.get("RANK", "0"))
+    if rank != 0:
+        return 0
+    wl = workload(args)
+    binary = reference_binary(wl.params)
+    cfg = describe(wl)
+    if binary is None:
+        print(json.dumps({"impl": "reference", "unavailable": "reference binary for this geometry not built"}))
+        return 0
+    pats = wl.patterns(args.seed)
+    text = wl.text(args.seed, pats)
+    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
+    nproc = max(1, min(cores, 64))
+    shard = min(32 << 20, (text.size - 65536) // nproc)
+    shards = line_shards(text, nproc, shard)
+    base, dirs = prepare_reference_dirs(binary, pats, text, shards)
+    try:
+        total = sum(n for _, n in dirs)
+        for _ in range(args.warmup):
+            run_reference_step(binary, dirs)
+        ts = [run_reference_step(binary, dirs) for _ in range(args.steps)]
+    finally:
+        shutil.rmtree(base, ignore_errors=True)
+    t = statistics.mean(ts)
+    value = total / t / 1e9
+    line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
+            "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": cfg,
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(dirs), "kind": "reference",
+                             "sample": f"{len(dirs)} processes x {shard / 2**20:.0f} MiB line-aligned shards "
+                                       f"({total / 2**30:.2f} GiB per step), filter from __bloom_filter_ cache"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---- our arm --------------------------------------------------------------------------------------------
+def main_ours(args):
+    import torch
+    import torch.distributed as dist
+
+    import ffbf_b200
+    from ffbf_b200 import Filter
+
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    torch.cuda.set_device(local)
+    dev = torch.device("cuda", local)
+    if world > 1:
+        from datetime import timedelta
+        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    wl = workload(args)
+    seed = args.seed + rank  # independent replicas
+    pats = wl.patterns(seed)
+    host = torch.empty(wl.text_bytes, dtype=torch.uint8, pin_memory=True)
+    text = host.numpy()
+    wl.text(seed, pats, out=text)
+    n = wl.text_bytes
+
+    f = Filter(wl.params, device=local)
+    f.add_patterns(pats)
+    d_text = torch.empty(n + 64, dtype=torch.uint8, device=dev)
+    d_text[:n].copy_(host, non_blocking=False)
+    torch.cuda.synchronize()
+    stream = torch.cuda.ExternalStream(f.stream, device=dev)
+
+    def step():
+        f.clear_ff()
+        f.process_device(d_text.data_ptr(), n)
+
+    sampler = ClockSampler(gpu_id_for(local))
+    sampler.start()
+    for _ in range(args.warmup):
+        step()
+        f.collect()
+    torch.cuda.synchronize()
+    barrier()
+    torch.cuda.synchronize()
+    launches0 = ffbf_b200.kernel_launches()
+    ev = [torch.cuda.Event(enable_timing=True) for _ in range(2 * args.steps)]
+    for i in range(args.steps):
+        ev[2 * i].record(stream)
+        step()
+        ev[2 * i + 1].record(stream)
+    stream.synchronize()
+    torch.cuda.synchronize()
+    barrier()
+    launches = ffbf_b200.kernel_launches() - launches0
+    per_step = [ev[2 * i].elapsed_time(ev[2 * i + 1]) for i in range(args.steps)]
+    total_ms = ev[0].elapsed_time(ev[-1])
+    total_ms = max_over_ranks(total_ms)
+    res = f.collect()
+
+    # end-to-end through the public API from pinned host memory
+    e2e_steps = args.e2e_steps or min(args.steps, 5)
+    barrier()
+    t0 = time.perf_counter()
+    d2h = 0
+    for _ in range(e2e_steps):
+        f.clear_ff()
+        r = f.process(text)
+        ids = f.filter_phrases()
+        off, pid = f.verify()
+        d2h += r.hit_offsets.size * 32 + ids.size * 8 + off.size * 12
+    torch.cuda.synchronize()
+    e2e_s = max_over_ranks(time.perf_counter() - t0)
+    clocks = sampler.stop()
+
+    value = world * n * args.steps / (total_ms * 1e-3) / 1e9
+    kernel_ms = statistics.mean(per_step)
+    peak, peak_kind = measured_peaks()
+    achieved = n / (kernel_ms * 1e-3) / 1e9
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+        "config": dict(describe(wl), parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                     "algorithmic_bytes_per_launch": n},
+        "e2e": {"value": world * n * e2e_steps / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": n,
+                "d2h_bytes_per_step": d2h // max(e2e_steps, 1),
+                "api": "ffbf_scan + ffbf_prune + ffbf_verify from pinned host memory"},
+        "gpu_launches": int(launches),
+        "clocks": clocks,
+        "results": {"hits": int(res.hit_offsets.size), "lines": int(res.line_start.size),
+                    "pruned_patterns": int(ids.size), "exact_matches": int(off.size)},
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline_single(wl, pats, text, args.cpu_sample)
+        except Exception as e:  # the baseline is reported, never required
+            line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
+                                    "sample": f"failed: {e}"}
+    f.close()
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+if __name__ == "__main__":
+    a = parse()
+    sys.exit(main_reference(a) if a.impl == "reference" else main_ours(a))

@@ -1,0 +1,653 @@
+// ffbf_kernels.cu -- FFBF device kernels other than the tuned scan: pattern line table and prefix
+// hashing (filter build), the generic scan, hit -> line resolution, feed-forward prune, ordered
+// compaction, the exact-verification hash table and byte compare, the filter cache codec and the
+// single-line test.
+#include <atomic>
+#include <climits>
+
+#include "ffbf_kernels.cuh"
+
+namespace ffbf {
+
+static std::atomic<uint64_t> g_launches{0};
+void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
+
+// ------------------------------------------------------------------------------------------------
+// Block-wide exclusive scan (THREADS a multiple of 32, <= 1024). `sh` holds THREADS/32 values.
+template <int THREADS, class T>
+__device__ __forceinline__ T block_excl_scan(T v, T* sh, T* total) {
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    T x = v;
+#pragma unroll
+    for (int d = 1; d < 32; d <<= 1) {
+        T y = __shfl_up_sync(0xffffffffu, x, d);
+        if (lane >= d) x += y;
+    }
+    if (lane == 31) sh[warp] = x;
+    __syncthreads();
+    if (warp == 0) {
+        T w = lane < THREADS / 32 ? sh[lane] : T(0);
+#pragma unroll
+        for (int d = 1; d < 32; d <<= 1) {
+            T y = __shfl_up_sync(0xffffffffu, w, d);
+            if (lane >= d) w += y;
+        }
+        if (lane < THREADS / 32) sh[lane] = w;
+    }
+    __syncthreads();
+    T before = warp ? sh[warp - 1] : T(0);
+    *total = sh[THREADS / 32 - 1];
+    __syncthreads();
+    return before + x - v;
+}
+
+// ------------------------------------------------------------------------------------------------
+// Ordered compaction, three phases: per-chunk counts, one-block exclusive scan of the counts, and an
+// ordered emit where every block writes the indices of its chunk in ascending order.
+constexpr int kCompThreads = 256;
+constexpr int kCompItems = 16;                                     // consecutive items per thread per round
+constexpr uint64_t kCompChunk = (uint64_t)kCompThreads * kCompItems * 16;  // items per block
+
+struct BytePred {
+    const uint8_t* p;
+    uint8_t b;
+    __device__ bool operator()(uint64_t i) const { return p[i] == b; }
+};
+struct FlagPred {
+    const uint8_t* p;
+    __device__ bool operator()(uint64_t i) const { return p[i] != 0; }
+};
+
+template <class Pred>
+__global__ void __launch_bounds__(kCompThreads) k_count(Pred pred, uint64_t n, uint64_t* counts) {
+    __shared__ uint64_t sh[kCompThreads / 32];
+    uint64_t lo = blockIdx.x * kCompChunk, hi = min(n, lo + kCompChunk);
+    uint64_t c = 0;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += kCompThreads) c += pred(i) ? 1 : 0;
+    uint64_t tot;
+    block_excl_scan<kCompThreads>(c, sh, &tot);
+    if (threadIdx.x == 0) counts[blockIdx.x] = tot;
+}
+
+// In place: counts[0..nb) -> exclusive prefix sums, counts[nb] = total. One block.
+template <class T>
+__global__ void __launch_bounds__(1024) k_scan_single(T* counts, uint64_t nb) {
+    __shared__ T sh[32];
+    T carry = 0;
+    for (uint64_t base = 0; base < nb; base += 1024) {
+        uint64_t i = base + threadIdx.x;
+        T v = i < nb ? counts[i] : T(0);
+        T tot;
+        T ex = block_excl_scan<1024>(v, sh, &tot);
+        if (i < nb) counts[i] = carry + ex;
+        carry += tot;
+    }
+    if (threadIdx.x == 0) counts[nb] = carry;
+}
+
+template <class Pred>
+__global__ void __launch_bounds__(kCompThreads) k_emit(Pred pred, uint64_t n, const uint64_t* offsets, uint64_t* out) {
+    __shared__ uint64_t sh[kCompThreads / 32];
+    uint64_t lo = blockIdx.x * kCompChunk, hi = min(n, lo + kCompChunk);
+    uint64_t base = offsets[blockIdx.x];
+    for (uint64_t r = lo; r < hi; r += (uint64_t)kCompThreads * kCompItems) {
+        uint64_t a = r + (uint64_t)threadIdx.x * kCompItems;
+        uint64_t b = min(hi, a + kCompItems);
+        uint64_t c = 0;
+        for (uint64_t i = a; i < b; i++) c += pred(i) ? 1 : 0;
+        uint64_t tot;
+        uint64_t pos = base + block_excl_scan<kCompThreads>(c, sh, &tot);
+        for (uint64_t i = a; i < b; i++)
+            if (pred(i)) out[pos++] = i;
+        base += tot;
+    }
+}
+
+uint64_t compact_blocks(uint64_t n) { return (n + kCompChunk - 1) / kCompChunk; }
+
+template <class Pred>
+static cudaError_t compact_count(Pred pred, uint64_t n, uint64_t* d_tmp, cudaStream_t st) {
+    uint64_t nb = compact_blocks(n);
+    if (nb == 0) return cudaMemsetAsync(d_tmp, 0, sizeof(uint64_t), st);
+    k_count<<<(unsigned)nb, kCompThreads, 0, st>>>(pred, n, d_tmp);
+    note_launches(1);
+    k_scan_single<uint64_t><<<1, 1024, 0, st>>>(d_tmp, nb);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+template <class Pred>
+static cudaError_t compact_emit(Pred pred, uint64_t n, uint64_t* d_out, const uint64_t* d_tmp, cudaStream_t st) {
+    uint64_t nb = compact_blocks(n);
+    if (nb == 0) return cudaSuccess;
+    k_emit<<<(unsigned)nb, kCompThreads, 0, st>>>(pred, n, d_tmp, d_out);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t count_bytes(const uint8_t* d_buf, uint64_t n, uint8_t byte, uint64_t* d_tmp, cudaStream_t st) {
+    return compact_count(BytePred{d_buf, byte}, n, d_tmp, st);
+}
+cudaError_t emit_bytes(const uint8_t* d_buf, uint64_t n, uint8_t byte, uint64_t* d_pos, const uint64_t* d_tmp,
+                       cudaStream_t st) {
+    return compact_emit(BytePred{d_buf, byte}, n, d_pos, d_tmp, st);
+}
+cudaError_t count_flags(const uint8_t* d_flags, uint64_t n, uint64_t* d_tmp, cudaStream_t st) {
+    return compact_count(FlagPred{d_flags}, n, d_tmp, st);
+}
+cudaError_t emit_flags(const uint8_t* d_flags, uint64_t n, uint64_t* d_out, const uint64_t* d_tmp, cudaStream_t st) {
+    return compact_emit(FlagPred{d_flags}, n, d_out, d_tmp, st);
+}
+
+// Line table of a pattern file from its newline positions: line i ends at nl[i] (or at n for a final
+// line without '\n') and starts one past the previous line's end.
+__global__ void k_lines(const uint64_t* nl, uint64_t m, uint64_t n, int tail, uint64_t* start, uint64_t* end) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    uint64_t cnt = m + (tail ? 1 : 0);
+    if (i >= cnt) return;
+    end[i] = i < m ? nl[i] : n;
+    start[i] = i == 0 ? 0 : nl[i - 1] + 1;
+}
+
+cudaError_t lines_from_newlines(const uint64_t* d_nl, uint64_t m, uint64_t n, int tail, uint64_t* d_start,
+                                uint64_t* d_end, cudaStream_t st) {
+    uint64_t cnt = m + (tail ? 1 : 0);
+    if (!cnt) return cudaSuccess;
+    k_lines<<<(unsigned)((cnt + 255) / 256), 256, 0, st>>>(d_nl, m, n, tail, d_start, d_end);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Filter build: one thread per pattern line. operator<< (ffbf.cpp:268-283) hashes the first LEN bytes
+// of a line at least LEN long and sets K bits in getHashValue order. The prefix hash is kept for the
+// feed-forward prune and for verification.
+__global__ void k_hash_patterns(const uint8_t* file, const uint64_t* start, const uint64_t* end, uint64_t npat,
+                                Geom g, uint64_t* hash, uint32_t* main_words, int set_bits) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= npat) return;
+    uint64_t s = start[i], e = end[i];
+    if (e - s < g.len) {
+        hash[i] = 0;
+        return;
+    }
+    uint64_t h = window_hash(file + s, g.len);
+    hash[i] = h;
+    if (set_bits)
+        for (uint32_t j = 0; j < g.k; j++) {
+            uint32_t b = bit_index<1>(g, h, j);
+            atomicOr(main_words + (b >> 5), 1u << (b & 31));
+        }
+}
+
+cudaError_t hash_patterns(const uint8_t* d_file, const uint64_t* d_start, const uint64_t* d_end, uint64_t npat,
+                          const Geom& g, uint64_t* d_hash, uint32_t* d_main, int set_bits, cudaStream_t st) {
+    if (!npat) return cudaSuccess;
+    k_hash_patterns<<<(unsigned)((npat + 255) / 256), 256, 0, st>>>(d_file, d_start, d_end, npat, g, d_hash, d_main,
+                                                                       set_bits);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Generic scan (any LEN 1..63, K, S, geometry). processFile (ffbf.cpp:310-392) restated per window:
+// the window ending at p is valid when its LEN bytes hold no '\n' (the reference resets the hash at
+// '\n' and tests only once LEN bytes followed); a valid window hits when its K main bits are set, and
+// then sets K feed-forward bits. Each CTA stages TILE bytes plus a 64-byte halo in shared memory; each
+// thread owns SEG consecutive window ends and rolls the hash over them after a LEN-byte warm-up.
+// The staged bytes are padded by 4 bytes after every 64 so that the threads' segments (64 bytes apart)
+// fall in different banks.
+__host__ __device__ __forceinline__ uint32_t pad_idx(uint32_t q) { return q + ((q >> 6) << 2); }
+
+size_t scan_smem_bytes(int cache_in_smem, const Geom& g) {
+    size_t text = pad_idx(kScanTile + kHalo) + 16;
+    size_t b = 2048 + 16 + ((text + 15) & ~(size_t)15);
+    if (cache_in_smem) b += g.cache_bits / 8;
+    return b;
+}
+
+__global__ void __launch_bounds__(kScanThreads) k_scan_generic(ScanArgs a) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint64_t* s_sbox = reinterpret_cast<uint64_t*>(smem);
+    long long* s_nl = reinterpret_cast<long long*>(smem + 2048);
+    uint8_t* s_text = smem + 2048 + 16;
+    const uint32_t text_bytes = (pad_idx(kScanTile + kHalo) + 16 + 15) & ~15u;
+    uint32_t* s_cache = reinterpret_cast<uint32_t*>(s_text + text_bytes);
+
+    const Geom g = a.g;
+    const uint32_t L = g.len;
+    const int tid = threadIdx.x;
+    for (int i = tid; i < 256; i += kScanThreads) s_sbox[i] = c_sbox[(i & 0x80) ? 0 : i];
+    if (a.cache_in_smem)
+        for (uint32_t w = tid; w < g.cache_bits / 32; w += kScanThreads) s_cache[w] = a.main_words[w];
+    const uint32_t* cache_words = a.cache_in_smem ? s_cache : a.main_words;
+
+    for (uint64_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+        __syncthreads();
+        const long long t0 = (long long)(tile * kScanTile);
+        for (int q = tid; q < (kScanTile + kHalo) / 4; q += kScanThreads) {
+            long long p = t0 - kHalo + 4LL * q;
+            uint32_t v;
+            if (p >= 0 && p + 4 <= (long long)a.n) {
+                v = __ldg(reinterpret_cast<const uint32_t*>(a.text + p));
+            } else {
+                v = 0;
+                for (int j = 0; j < 4; j++) {
+                    long long pj = p + j;
+                    uint32_t b = (pj < 0 || pj >= (long long)a.n) ? 0x0Au : a.text[pj];
+                    v |= b << (8 * j);
+                }
+            }
+            *reinterpret_cast<uint32_t*>(s_text + pad_idx(4 * q)) = v;
+        }
+        if (tid == 0) {
+            s_nl[0] = LLONG_MAX;
+            s_nl[1] = -1;
+        }
+        __syncthreads();
+
+        const long long seg0 = t0 + (long long)tid * kScanSeg;
+        long long my_first = LLONG_MAX, my_last = -1;
+        if (seg0 < (long long)a.n) {
+            const long long seg1 = min(seg0 + kScanSeg, (long long)a.n);
+            // staged byte of text position p: s_text[pad_idx(p - (t0 - kHalo))]
+            const long long off = kHalo - t0;
+            uint64_t h = 0;
+            uint32_t run = 0;
+            for (long long p = seg0 - L; p < seg0; p++) {
+                uint32_t c = s_text[pad_idx((uint32_t)(p + off))];
+                h = rol64(h, 1) ^ s_sbox[c];
+                run = c == 0x0Au ? 0u : min(run + 1u, L);
+            }
+            for (long long p = seg0; p < seg1; p++) {
+                uint32_t c = s_text[pad_idx((uint32_t)(p + off))];
+                uint32_t co = s_text[pad_idx((uint32_t)(p - L + off))];
+                h = rol64(h, 1) ^ s_sbox[c] ^ rol64(s_sbox[co], L);
+                if (c == 0x0Au) {
+                    run = 0;
+                    if (my_first == LLONG_MAX) my_first = p;
+                    my_last = p;
+                    continue;
+                }
+                run = min(run + 1u, L);
+                if (run < L) continue;
+                bool hit = true;
+                for (uint32_t i = 0; i < g.k && hit; i++) {
+                    uint32_t b = bit_index<1>(g, h, i);
+                    hit = test_bit(i < g.s ? cache_words : a.main_words, b);
+                }
+                if (hit) {
+                    set_all<2>(g, a.ff_words, h);
+                    uint32_t slot = atomicAdd(a.counters + CNT_HITS, 1u);
+                    if (slot < a.hits_cap) a.hits[slot] = HitRec{(uint64_t)(p + 1 - L), h};
+                }
+            }
+        }
+        if (my_first != LLONG_MAX) atomicMin(s_nl + 0, my_first);
+        if (my_last >= 0) atomicMax(s_nl + 1, my_last);
+        __syncthreads();
+        if (tid == 0) {
+            a.tile_first_nl[tile] = s_nl[0];
+            a.tile_last_nl[tile] = s_nl[1];
+        }
+    }
+}
+
+int scan_generic_grid(const Geom& g, int cache_in_smem, uint64_t ntiles) {
+    size_t smem = scan_smem_bytes(cache_in_smem, g);
+    if (cudaFuncSetAttribute(k_scan_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)
+        return 0;
+    int dev = 0, sms = 0, per = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, k_scan_generic, kScanThreads, smem) != cudaSuccess) return 0;
+    uint64_t grid = (uint64_t)sms * (per > 0 ? per : 1);
+    return (int)(grid < ntiles ? grid : (ntiles ? ntiles : 1));
+}
+
+cudaError_t scan_generic(const ScanArgs& a, int grid, cudaStream_t st) {
+    size_t smem = scan_smem_bytes(a.cache_in_smem, a.g);
+    cudaError_t e = cudaFuncSetAttribute(k_scan_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    if (a.ntiles == 0) return cudaSuccess;
+    k_scan_generic<<<grid, kScanThreads, smem, st>>>(a);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Hit -> line span. Tile summaries give, for every tile, the last '\n' before it and the first '\n'
+// after it, so each hit searches at most one tile in each direction.
+__global__ void __launch_bounds__(1024) k_tile_nl_scan(const long long* first, const long long* last,
+                                                       long long* prev_nl, long long* next_nl, uint64_t nt) {
+    // prev_nl[t] = max(last[0..t)), next_nl[t] = min(first(t..nt)). One block; per-thread ranges.
+    __shared__ long long sh[1024];
+    const uint64_t per = (nt + 1023) / 1024;
+    const uint64_t lo = min(nt, threadIdx.x * per), hi = min(nt, lo + per);
+    long long m = -1;
+    for (uint64_t t = lo; t < hi; t++) m = max(m, last[t]);
+    sh[threadIdx.x] = m;
+    __syncthreads();
+    long long before = -1;
+    for (unsigned u = 0; u < threadIdx.x; u++) before = max(before, sh[u]);
+    for (uint64_t t = lo; t < hi; t++) {
+        prev_nl[t] = before;
+        before = max(before, last[t]);
+    }
+    __syncthreads();
+    long long f = LLONG_MAX;
+    for (uint64_t t = lo; t < hi; t++) f = min(f, first[t]);
+    sh[threadIdx.x] = f;
+    __syncthreads();
+    long long after = LLONG_MAX;
+    for (unsigned u = threadIdx.x + 1; u < 1024; u++) after = min(after, sh[u]);
+    for (uint64_t t = hi; t > lo; t--) {
+        next_nl[t - 1] = after;
+        after = min(after, first[t - 1]);
+    }
+}
+
+__global__ void k_resolve(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
+                          const long long* prev_nl, const long long* next_nl, HitLine* out) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nhits) return;
+    const uint64_t w = hits[j].off;
+    uint64_t s = 0;
+    if (w > 0) {
+        uint64_t tb = (w - 1) / kScanTile;
+        long long p = (long long)w - 1, lo = (long long)(tb * kScanTile);
+        while (p >= lo && text[p] != '\n') p--;
+        if (p >= lo) s = (uint64_t)p + 1;
+        else s = (uint64_t)(prev_nl[tb] + 1);
+    }
+    uint64_t e = n;
+    uint64_t q = w + len;
+    if (q < n) {
+        uint64_t te = q / kScanTile;
+        uint64_t hi = min(n, (te + 1) * (uint64_t)kScanTile);
+        while (q < hi && text[q] != '\n') q++;
+        if (q < hi) e = q;
+        else e = next_nl[te] == LLONG_MAX ? n : (uint64_t)next_nl[te];
+    }
+    out[j] = HitLine{s, e};
+}
+
+cudaError_t resolve_lines(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
+                          const long long* tile_first, const long long* tile_last, long long* prev_nl,
+                          long long* next_nl, uint64_t ntiles, HitLine* out, cudaStream_t st) {
+    if (ntiles) {
+        k_tile_nl_scan<<<1, 1024, 0, st>>>(tile_first, tile_last, prev_nl, next_nl, ntiles);
+        note_launches(1);
+    }
+    if (nhits) {
+        k_resolve<<<(nhits + 255) / 256, 256, 0, st>>>(text, n, len, hits, nhits, prev_nl, next_nl, out);
+        note_launches(1);
+    }
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Feed-forward prune (filterPhrases, ffbf.cpp:394-485): a line survives when it is >= LEN bytes and its
+// prefix window's K feed-forward bits (getHashValue_2 order) are set.
+__global__ void k_prune(const uint64_t* start, const uint64_t* end, const uint64_t* hash, uint64_t npat, Geom g,
+                        const uint32_t* ff, uint8_t* flags) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= npat) return;
+    flags[i] = (end[i] - start[i] >= g.len) && check_all<2>(g, ff, hash[i]);
+}
+
+cudaError_t prune_flags(const uint64_t* d_start, const uint64_t* d_end, const uint64_t* d_hash, uint64_t npat,
+                        const Geom& g, const uint32_t* d_ff, uint8_t* d_flags, cudaStream_t st) {
+    if (!npat) return cudaSuccess;
+    k_prune<<<(unsigned)((npat + 255) / 256), 256, 0, st>>>(d_start, d_end, d_hash, npat, g, d_ff, d_flags);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Exact verification. Open-addressing multimap keyed by the pruned patterns' 64-bit prefix hash; every
+// pattern gets its own slot (several patterns may share a prefix). Slots are claimed with atomicCAS on
+// the value array (empty = 0xffffffff); lookups run in a later kernel.
+__device__ __forceinline__ uint64_t mix64(uint64_t x) {
+    x ^= x >> 33;
+    x *= 0xff51afd7ed558ccdull;
+    x ^= x >> 33;
+    x *= 0xc4ceb9fe1a85ec53ull;
+    return x ^ (x >> 33);
+}
+
+__global__ void k_table_build(const uint64_t* ids, uint64_t nids, const uint64_t* hash, uint64_t* keys,
+                              uint32_t* vals, uint64_t mask, uint32_t* counters) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= nids) return;
+    uint32_t id = (uint32_t)ids[i];
+    uint64_t key = hash[id];
+    uint64_t slot = mix64(key) & mask;
+    for (uint64_t probe = 0; probe <= mask; probe++) {
+        uint32_t old = atomicCAS(vals + slot, 0xffffffffu, id);
+        if (old == 0xffffffffu) {
+            keys[slot] = key;
+            return;
+        }
+        slot = (slot + 1) & mask;
+    }
+    atomicOr(counters + CNT_ERROR, 1u);  // table full: cannot happen with size >= 2 * nids
+}
+
+cudaError_t table_build(const uint64_t* d_ids, uint64_t nids, const uint64_t* d_hash, uint64_t* d_keys,
+                        uint32_t* d_vals, uint64_t mask, uint32_t* d_counters, cudaStream_t st) {
+    if (!nids) return cudaSuccess;
+    k_table_build<<<(unsigned)((nids + 255) / 256), 256, 0, st>>>(d_ids, nids, d_hash, d_keys, d_vals, mask,
+                                                                    d_counters);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// One thread per hit window: look its hash up, byte-compare every candidate pattern at the window start.
+__global__ void k_verify(const HitRec* hits, uint32_t nhits, const uint8_t* text, uint64_t n, const uint64_t* keys,
+                         const uint32_t* vals, uint64_t mask, const uint8_t* pat, const uint64_t* pstart,
+                         const uint64_t* pend, uint64_t* m_off, uint32_t* m_pid, uint32_t cap, uint32_t* counters) {
+    uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
+    if (j >= nhits) return;
+    const uint64_t w = hits[j].off, h = hits[j].h;
+    uint64_t slot = mix64(h) & mask;
+    for (uint64_t probe = 0; probe <= mask; probe++) {
+        uint32_t id = vals[slot];
+        if (id == 0xffffffffu) break;
+        if (keys[slot] == h) {
+            uint64_t ps = pstart[id], pl = pend[id] - ps;
+            if (w + pl <= n) {
+                const uint8_t* t = text + w;
+                const uint8_t* q = pat + ps;
+                uint64_t k = 0;
+                // 8-byte compares while both sides allow an aligned-free byte gather
+                while (k + 8 <= pl) {
+                    uint64_t x = 0, y = 0;
+#pragma unroll
+                    for (int b = 0; b < 8; b++) {
+                        x |= (uint64_t)t[k + b] << (8 * b);
+                        y |= (uint64_t)q[k + b] << (8 * b);
+                    }
+                    if (x != y) break;
+                    k += 8;
+                }
+                while (k < pl && t[k] == q[k]) k++;
+                if (k == pl) {
+                    uint32_t o = atomicAdd(counters + CNT_MATCHES, 1u);
+                    if (o < cap) {
+                        m_off[o] = w;
+                        m_pid[o] = id;
+                    }
+                }
+            }
+        }
+        slot = (slot + 1) & mask;
+    }
+}
+
+cudaError_t verify_hits(const HitRec* hits, uint32_t nhits, const uint8_t* text, uint64_t n, const uint64_t* d_keys,
+                        const uint32_t* d_vals, uint64_t mask, const uint8_t* d_pat, const uint64_t* d_start,
+                        const uint64_t* d_end, uint64_t* d_match_off, uint32_t* d_match_pid, uint32_t match_cap,
+                        uint32_t* d_counters, cudaStream_t st) {
+    if (!nhits) return cudaSuccess;
+    k_verify<<<(nhits + 255) / 256, 256, 0, st>>>(hits, nhits, text, n, d_keys, d_vals, mask, d_pat, d_start, d_end,
+                                                   d_match_off, d_match_pid, match_cap, d_counters);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// Filter cache file codec. loadFilterFromFile (ffbf.cpp:487-506) accumulates uint32 deltas (wrapping)
+// and sets each running sum; saveFilterToFile (ffbf.cpp:508-527) writes the gaps between set bits.
+constexpr int kCodecThreads = 256;
+constexpr uint64_t kCodecChunk = 65536;
+
+__global__ void __launch_bounds__(kCodecThreads) k_delta_block_sums(const uint32_t* d, uint64_t nd, uint32_t* sums) {
+    __shared__ uint32_t sh[kCodecThreads / 32];
+    uint64_t lo = blockIdx.x * kCodecChunk, hi = min(nd, lo + kCodecChunk);
+    uint32_t s = 0;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += kCodecThreads) s += d[i];
+    uint32_t tot;
+    block_excl_scan<kCodecThreads>(s, sh, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kCodecThreads) k_delta_apply(const uint32_t* d, uint64_t nd, const uint32_t* offs,
+                                                                uint32_t nbits, uint32_t* idx, uint32_t* counters) {
+    __shared__ uint32_t sh[kCodecThreads / 32];
+    constexpr int items = 16;
+    uint64_t lo = blockIdx.x * kCodecChunk, hi = min(nd, lo + kCodecChunk);
+    uint32_t base = offs[blockIdx.x];
+    for (uint64_t r = lo; r < hi; r += (uint64_t)kCodecThreads * items) {
+        uint64_t a = r + (uint64_t)threadIdx.x * items, b = min(hi, a + items);
+        uint32_t s = 0;
+        for (uint64_t i = a; i < b; i++) s += d[i];
+        uint32_t tot;
+        uint32_t run = base + block_excl_scan<kCodecThreads>(s, sh, &tot);
+        for (uint64_t i = a; i < b; i++) {
+            run += d[i];
+            idx[i] = run;
+            if (run >= nbits) atomicOr(counters + CNT_ERROR, 2u);
+        }
+        base += tot;
+    }
+}
+
+cudaError_t filter_decode(const uint32_t* d_deltas, uint64_t nd, uint32_t nbits, uint32_t* d_idx, uint64_t* d_tmp,
+                          uint32_t* d_counters, cudaStream_t st) {
+    if (!nd) return cudaSuccess;
+    uint64_t nb = (nd + kCodecChunk - 1) / kCodecChunk;
+    uint32_t* sums = reinterpret_cast<uint32_t*>(d_tmp);
+    k_delta_block_sums<<<(unsigned)nb, kCodecThreads, 0, st>>>(d_deltas, nd, sums);
+    note_launches(1);
+    k_scan_single<uint32_t><<<1, 1024, 0, st>>>(sums, nb);
+    note_launches(1);
+    k_delta_apply<<<(unsigned)nb, kCodecThreads, 0, st>>>(d_deltas, nd, sums, nbits, d_idx, d_counters);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+__global__ void k_set_indices(const uint32_t* idx, uint64_t nd, uint32_t* words) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= nd) return;
+    uint32_t b = idx[i];
+    atomicOr(words + (b >> 5), 1u << (b & 31));
+}
+
+cudaError_t filter_set_indices(const uint32_t* d_idx, uint64_t nd, uint32_t* d_main, cudaStream_t st) {
+    if (!nd) return cudaSuccess;
+    k_set_indices<<<(unsigned)((nd + 255) / 256), 256, 0, st>>>(d_idx, nd, d_main);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// Encode: popcount per word chunk, scan, then emit ascending set-bit indices as deltas.
+constexpr uint64_t kEncChunkWords = 16384;
+
+__global__ void __launch_bounds__(kCodecThreads) k_popc_blocks(const uint32_t* w, uint32_t nwords, uint64_t* sums) {
+    __shared__ uint64_t sh[kCodecThreads / 32];
+    uint64_t lo = blockIdx.x * kEncChunkWords, hi = min((uint64_t)nwords, lo + kEncChunkWords);
+    uint64_t s = 0;
+    for (uint64_t i = lo + threadIdx.x; i < hi; i += kCodecThreads) s += __popc(w[i]);
+    uint64_t tot;
+    block_excl_scan<kCodecThreads>(s, sh, &tot);
+    if (threadIdx.x == 0) sums[blockIdx.x] = tot;
+}
+
+__global__ void __launch_bounds__(kCodecThreads) k_emit_bits(const uint32_t* w, uint32_t nwords, const uint64_t* offs,
+                                                              uint32_t* out) {
+    __shared__ uint64_t sh[kCodecThreads / 32];
+    uint64_t lo = blockIdx.x * kEncChunkWords, hi = min((uint64_t)nwords, lo + kEncChunkWords);
+    uint64_t base = offs[blockIdx.x];
+    for (uint64_t r = lo; r < hi; r += kCodecThreads) {
+        uint64_t i = r + threadIdx.x;
+        uint32_t v = i < hi ? w[i] : 0u;
+        uint64_t tot;
+        uint64_t pos = base + block_excl_scan<kCodecThreads>((uint64_t)__popc(v), sh, &tot);
+        while (v) {
+            uint32_t b = __ffs(v) - 1;
+            v &= v - 1;
+            out[pos++] = (uint32_t)(i * 32 + b);
+        }
+        base += tot;
+    }
+}
+
+__global__ void k_to_deltas(const uint32_t* idx, uint64_t n, uint32_t* out) {
+    uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out[i] = idx[i] - (i ? idx[i - 1] : 0u);
+}
+
+uint64_t enc_blocks(uint32_t nwords) { return (nwords + kEncChunkWords - 1) / kEncChunkWords; }
+uint64_t decode_blocks(uint64_t nd) { return (nd + kCodecChunk - 1) / kCodecChunk; }
+
+cudaError_t filter_count(const uint32_t* d_main, uint32_t nwords, uint64_t* d_tmp, cudaStream_t st) {
+    uint64_t nb = enc_blocks(nwords);
+    k_popc_blocks<<<(unsigned)nb, kCodecThreads, 0, st>>>(d_main, nwords, d_tmp);
+    note_launches(1);
+    k_scan_single<uint64_t><<<1, 1024, 0, st>>>(d_tmp, nb);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t filter_encode(const uint32_t* d_main, uint32_t nwords, const uint64_t* d_tmp, uint32_t* d_idx,
+                          cudaStream_t st) {
+    uint64_t nb = enc_blocks(nwords);
+    k_emit_bits<<<(unsigned)nb, kCodecThreads, 0, st>>>(d_main, nwords, d_tmp, d_idx);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+cudaError_t filter_deltas(const uint32_t* d_idx, uint64_t n, uint32_t* d_out, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    k_to_deltas<<<(unsigned)((n + 255) / 256), 256, 0, st>>>(d_idx, n, d_out);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// ------------------------------------------------------------------------------------------------
+// operator[] (ffbf.cpp:285-308): one string, no newline handling, first hitting window wins.
+__global__ void k_test_line(const uint8_t* s, uint64_t n, Geom g, const uint32_t* main_words, uint32_t* out) {
+    if (threadIdx.x != 0 || blockIdx.x != 0) return;
+    uint32_t res = 0;
+    if (n >= g.len) {
+        uint64_t h = 0;
+        for (uint64_t p = 0; p < n && !res; p++) {
+            h = rol64(h, 1) ^ sbox_of(s[p]);
+            if (p >= g.len) h ^= rol64(sbox_of(s[p - g.len]), g.len);
+            if (p + 1 >= g.len && check_all<1>(g, main_words, h)) res = 1;
+        }
+    }
+    *out = res;
+}
+
+cudaError_t test_line(const uint8_t* d_line, uint64_t n, const Geom& g, const uint32_t* d_main, uint32_t* d_out,
+                      cudaStream_t st) {
+    k_test_line<<<1, 32, 0, st>>>(d_line, n, g, d_main, d_out);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+}  // namespace ffbf

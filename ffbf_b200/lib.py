@@ -1,0 +1,324 @@
+"""Python access to the C ABI in include/ffbf.h (ffbf_b200/_lib/libffbf.so).
+
+`Filter` mirrors efficient/ffbf's Filter<H, LEN> (src/rabin-karp/ffbf.h:43-93) member for member:
+
+    reference (C++)                         here
+    filter << phrase  (per getline line)    Filter.add_patterns(file_bytes)
+    filter[line]                            Filter.test_line(line)
+    processFile(fd)                         Filter.process(text) / Filter.process_device(ptr, n)
+    filterPhrases(pfd, out, outIndex)       Filter.filter_phrases() + Filter.format_pruned()
+    loadFilterFromFile(fd)                  Filter.load_filter(data) / load_filter_from_file(path)
+    saveFilterToFile(fd)                    Filter.save_filter() / save_filter_to_file(path)
+
+Failures raise FFBFError (the reference throws FilterError, ffbf.h:31-41) carrying the C status and
+ffbf_last_error(). There is no fallback: if the native library is missing this module raises on load.
+"""
+import ctypes
+import os
+from dataclasses import dataclass
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libffbf.so")
+
+# processFile and filterPhrases read() 512 KiB at a time (src/rabin-karp/ffbf.cpp:313,397); a regular
+# file returns full chunks, which is what the output rules depend on.
+DEFAULT_CHUNK = 512 * 1024
+
+STATUS = {0: "FFBF_OK", 1: "FFBF_EINVAL", 2: "FFBF_ENOMEM_DEVICE", 3: "FFBF_EIO", 4: "FFBF_ETIMEOUT",
+          5: "FFBF_ECUDA", 6: "FFBF_ESTATE", 7: "FFBF_ENOMEM_HOST"}
+
+EXPORTED = [
+    "ffbf_params_default", "ffbf_create", "ffbf_destroy", "ffbf_last_error", "ffbf_status_string",
+    "ffbf_set_hbm_budget", "ffbf_set_patterns", "ffbf_build", "ffbf_add_patterns", "ffbf_load_filter",
+    "ffbf_save_filter", "ffbf_load_filter_file", "ffbf_save_filter_file", "ffbf_scan", "ffbf_scan_device",
+    "ffbf_scan_collect", "ffbf_format_lines", "ffbf_prune", "ffbf_format_pruned", "ffbf_verify",
+    "ffbf_test_line", "ffbf_clear_ff", "ffbf_get_filters", "ffbf_filter_bytes", "ffbf_free", "ffbf_format_spans",
+    "ffbf_stream", "ffbf_kernel_launches",
+]
+
+
+class FFBFError(RuntimeError):
+    def __init__(self, status, message):
+        super().__init__(f"{STATUS.get(status, status)}: {message}")
+        self.status = status
+        self.message = message
+
+
+class Params(ctypes.Structure):
+    """ffbf_params: len=DEF_PATT_LEN, k=DEF_K, s=DEF_S, cache_bits=DEF_CACHE_SIZE, ext_bits=DEF_EXT_SIZE."""
+    _fields_ = [("len", ctypes.c_uint32), ("k", ctypes.c_uint32), ("s", ctypes.c_uint32),
+                ("reserved", ctypes.c_uint32), ("cache_bits", ctypes.c_uint64), ("ext_bits", ctypes.c_uint64)]
+
+    def __init__(self, len=19, k=5, s=2, cache_bits=1 << 24, ext_bits=1 << 28):
+        super().__init__(len, k, s, 0, cache_bits, ext_bits)
+
+    @property
+    def nbits(self):
+        return self.cache_bits + self.ext_bits
+
+    def as_tuple(self):
+        return (self.len, self.k, self.s, self.cache_bits, self.ext_bits)
+
+    def __repr__(self):
+        return f"Params(len={self.len}, k={self.k}, s={self.s}, cache_bits={self.cache_bits:#x}, ext_bits={self.ext_bits:#x})"
+
+
+class _ScanResult(ctypes.Structure):
+    _fields_ = [("text_len", ctypes.c_uint64), ("n_hits", ctypes.c_uint64),
+                ("hit_offsets", ctypes.POINTER(ctypes.c_uint64)), ("n_lines", ctypes.c_uint64),
+                ("line_start", ctypes.POINTER(ctypes.c_uint64)), ("line_end", ctypes.POINTER(ctypes.c_uint64))]
+
+
+class _PruneResult(ctypes.Structure):
+    _fields_ = [("n_ids", ctypes.c_uint64), ("ids", ctypes.POINTER(ctypes.c_uint64))]
+
+
+class _Matches(ctypes.Structure):
+    _fields_ = [("n", ctypes.c_uint64), ("offsets", ctypes.POINTER(ctypes.c_uint64)),
+                ("pattern_ids", ctypes.POINTER(ctypes.c_uint64))]
+
+
+_lib = None
+
+
+def load_library(path=LIB_PATH):
+    """Loads libffbf.so once. Raises FileNotFoundError when it has not been built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    if not os.path.exists(path):
+        raise FileNotFoundError(f"{path} is missing: build it with `python -m ffbf_b200.build`")
+    lib = ctypes.CDLL(path)
+    P = ctypes.POINTER
+    u8p, vp, sz = P(ctypes.c_uint8), ctypes.c_void_p, ctypes.c_size_t
+    sig = {
+        "ffbf_params_default": (ctypes.c_int, [P(Params)]),
+        "ffbf_create": (ctypes.c_int, [P(Params), ctypes.c_int, P(vp)]),
+        "ffbf_destroy": (None, [vp]),
+        "ffbf_last_error": (ctypes.c_char_p, [vp]),
+        "ffbf_status_string": (ctypes.c_char_p, [ctypes.c_int]),
+        "ffbf_set_hbm_budget": (ctypes.c_int, [vp, ctypes.c_uint64]),
+        "ffbf_set_patterns": (ctypes.c_int, [vp, vp, sz]),
+        "ffbf_build": (ctypes.c_int, [vp]),
+        "ffbf_add_patterns": (ctypes.c_int, [vp, vp, sz]),
+        "ffbf_load_filter": (ctypes.c_int, [vp, vp, sz]),
+        "ffbf_save_filter": (ctypes.c_int, [vp, P(u8p), P(sz)]),
+        "ffbf_load_filter_file": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "ffbf_save_filter_file": (ctypes.c_int, [vp, ctypes.c_char_p]),
+        "ffbf_scan": (ctypes.c_int, [vp, vp, sz, P(_ScanResult)]),
+        "ffbf_scan_device": (ctypes.c_int, [vp, vp, sz]),
+        "ffbf_scan_collect": (ctypes.c_int, [vp, P(_ScanResult)]),
+        "ffbf_format_lines": (ctypes.c_int, [vp, vp, sz, sz, P(u8p), P(sz)]),
+        "ffbf_prune": (ctypes.c_int, [vp, P(_PruneResult)]),
+        "ffbf_format_pruned": (ctypes.c_int, [vp, sz, P(u8p), P(sz), P(u8p), P(sz)]),
+        "ffbf_verify": (ctypes.c_int, [vp, P(_Matches)]),
+        "ffbf_test_line": (ctypes.c_int, [vp, vp, sz, P(ctypes.c_int)]),
+        "ffbf_clear_ff": (ctypes.c_int, [vp]),
+        "ffbf_get_filters": (ctypes.c_int, [vp, vp, vp]),
+        "ffbf_filter_bytes": (ctypes.c_uint64, [vp]),
+        "ffbf_free": (None, [vp]),
+        "ffbf_format_spans": (ctypes.c_int, [vp, sz, vp, vp, sz, sz, P(u8p), P(sz)]),
+        "ffbf_stream": (vp, [vp]),
+        "ffbf_kernel_launches": (ctypes.c_uint64, []),
+    }
+    for name, (res, args) in sig.items():
+        fn = getattr(lib, name)
+        fn.restype = res
+        fn.argtypes = args
+    _lib = lib
+    return lib
+
+
+def _buf(data):
+    """(pointer, length, keepalive) for bytes / bytearray / numpy uint8 data without copying numpy."""
+    if isinstance(data, np.ndarray):
+        a = np.ascontiguousarray(data, dtype=np.uint8)
+        return a.ctypes.data_as(ctypes.c_void_p), a.nbytes, a
+    if isinstance(data, (bytes, bytearray, memoryview)):
+        a = np.frombuffer(bytes(data) if isinstance(data, memoryview) else data, dtype=np.uint8)
+        return (a.ctypes.data_as(ctypes.c_void_p) if a.size else None), a.size, a
+    raise TypeError(f"expected bytes or a uint8 array, got {type(data).__name__}")
+
+
+def _arr(ptr, n):
+    if n == 0:
+        return np.zeros(0, dtype=np.uint64)
+    return np.ctypeslib.as_array(ptr, shape=(n,)).copy()
+
+
+def _take_bytes(lib, p, n):
+    try:
+        return ctypes.string_at(p, n.value) if n.value else b""
+    finally:
+        lib.ffbf_free(ctypes.cast(p, ctypes.c_void_p))
+
+
+def kernel_launches():
+    """Kernels the library has launched in this process so far."""
+    return int(load_library().ffbf_kernel_launches())
+
+
+def format_spans(buf, starts, ends, chunk=DEFAULT_CHUNK):
+    """ffbf_format_spans: the reference's stdout bytes for the given flagged line spans of `buf` (host only)."""
+    lib = load_library()
+    p, n, keep = _buf(buf)
+    st = np.ascontiguousarray(starts, dtype=np.uint64)
+    en = np.ascontiguousarray(ends, dtype=np.uint64)
+    out, m = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+    rc = lib.ffbf_format_spans(p, n, st.ctypes.data_as(ctypes.c_void_p), en.ctypes.data_as(ctypes.c_void_p), st.size,
+                               chunk, ctypes.byref(out), ctypes.byref(m))
+    if rc != 0:
+        raise FFBFError(rc, "ffbf_format_spans rejected its arguments")
+    return _take_bytes(lib, out, m)
+
+
+@dataclass
+class ScanOutput:
+    text_len: int
+    hit_offsets: np.ndarray  # uint64, ascending window start offsets
+    line_start: np.ndarray   # uint64, flagged lines in text order
+    line_end: np.ndarray     # uint64, exclusive, excludes the '\n'
+
+
+class Filter:
+    """One device-resident pair of bit arrays (main + feed-forward) with the reference's operations."""
+
+    def __init__(self, params=None, device=0):
+        self._lib = load_library()
+        self.params = params if params is not None else Params()
+        h = ctypes.c_void_p()
+        st = self._lib.ffbf_create(ctypes.byref(self.params), device, ctypes.byref(h))
+        if st != 0:
+            raise FFBFError(st, "ffbf_create failed (bad geometry or no usable CUDA device)")
+        self._h = h
+
+    # -- plumbing -----------------------------------------------------------------------------
+    def _check(self, st):
+        if st != 0:
+            raise FFBFError(st, self._lib.ffbf_last_error(self._h).decode(errors="replace"))
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ffbf_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def filter_bytes(self):
+        return int(self._lib.ffbf_filter_bytes(self._h))
+
+    @property
+    def stream(self):
+        """The context's cudaStream_t as an integer handle (e.g. for torch.cuda.ExternalStream)."""
+        return int(self._lib.ffbf_stream(self._h) or 0)
+
+    def set_hbm_budget(self, nbytes):
+        self._check(self._lib.ffbf_set_hbm_budget(self._h, nbytes))
+
+    # -- build ---------------------------------------------------------------------------------
+    def set_patterns(self, file_bytes):
+        p, n, keep = _buf(file_bytes)
+        self._check(self._lib.ffbf_set_patterns(self._h, p, n))
+
+    def build(self):
+        self._check(self._lib.ffbf_build(self._h))
+
+    def add_patterns(self, file_bytes):
+        """main()'s getline loop of `filter << phrase` (ffbf.cpp:556-571)."""
+        p, n, keep = _buf(file_bytes)
+        self._check(self._lib.ffbf_add_patterns(self._h, p, n))
+
+    def load_filter(self, data):
+        p, n, keep = _buf(data)
+        self._check(self._lib.ffbf_load_filter(self._h, p, n))
+
+    def save_filter(self):
+        out, n = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+        self._check(self._lib.ffbf_save_filter(self._h, ctypes.byref(out), ctypes.byref(n)))
+        return _take_bytes(self._lib, out, n)
+
+    def load_filter_from_file(self, path):
+        self._check(self._lib.ffbf_load_filter_file(self._h, os.fsencode(path)))
+
+    def save_filter_to_file(self, path):
+        self._check(self._lib.ffbf_save_filter_file(self._h, os.fsencode(path)))
+
+    # -- scan ----------------------------------------------------------------------------------
+    def _result(self, r):
+        return ScanOutput(int(r.text_len), _arr(r.hit_offsets, r.n_hits), _arr(r.line_start, r.n_lines),
+                          _arr(r.line_end, r.n_lines))
+
+    def process(self, text):
+        """processFile over a host text image."""
+        p, n, keep = _buf(text)
+        r = _ScanResult()
+        self._check(self._lib.ffbf_scan(self._h, p, n, ctypes.byref(r)))
+        return self._result(r)
+
+    def process_device(self, dev_ptr, n):
+        """Enqueues the scan of n bytes already on the device (16-byte aligned pointer)."""
+        self._check(self._lib.ffbf_scan_device(self._h, ctypes.c_void_p(dev_ptr), n))
+
+    def collect(self):
+        r = _ScanResult()
+        self._check(self._lib.ffbf_scan_collect(self._h, ctypes.byref(r)))
+        return self._result(r)
+
+    def format_lines(self, text, chunk=DEFAULT_CHUNK):
+        """The bytes processFile writes to stdout for the last scan."""
+        p, n, keep = _buf(text)
+        out, m = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+        self._check(self._lib.ffbf_format_lines(self._h, p, n, chunk, ctypes.byref(out), ctypes.byref(m)))
+        return _take_bytes(self._lib, out, m)
+
+    # -- feed-forward prune and verification ---------------------------------------------------
+    def filter_phrases(self):
+        """Ascending 0-based line numbers of the patterns that pass the feed-forward filter."""
+        r = _PruneResult()
+        self._check(self._lib.ffbf_prune(self._h, ctypes.byref(r)))
+        return _arr(r.ids, r.n_ids)
+
+    def format_pruned(self, chunk=DEFAULT_CHUNK):
+        """(pruned pattern file, __index_ file) bytes for the last filter_phrases()."""
+        o, on = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+        i, inn = ctypes.POINTER(ctypes.c_uint8)(), ctypes.c_size_t()
+        self._check(self._lib.ffbf_format_pruned(self._h, chunk, ctypes.byref(o), ctypes.byref(on), ctypes.byref(i),
+                                                 ctypes.byref(inn)))
+        return _take_bytes(self._lib, o, on), _take_bytes(self._lib, i, inn)
+
+    def verify(self):
+        """Exact (offset, pattern id) pairs, sorted."""
+        m = _Matches()
+        self._check(self._lib.ffbf_verify(self._h, ctypes.byref(m)))
+        return _arr(m.offsets, m.n), _arr(m.pattern_ids, m.n)
+
+    def test_line(self, line):
+        """operator[] (ffbf.cpp:285-308)."""
+        p, n, keep = _buf(line)
+        hit = ctypes.c_int()
+        self._check(self._lib.ffbf_test_line(self._h, p, n, ctypes.byref(hit)))
+        return bool(hit.value)
+
+    def clear_ff(self):
+        self._check(self._lib.ffbf_clear_ff(self._h))
+
+    def get_filters(self):
+        nb = self.filter_bytes
+        main = np.zeros(nb, dtype=np.uint8)
+        ff = np.zeros(nb, dtype=np.uint8)
+        self._check(self._lib.ffbf_get_filters(self._h, main.ctypes.data_as(ctypes.c_void_p),
+                                               ff.ctypes.data_as(ctypes.c_void_p)))
+        return main, ff

@@ -1,0 +1,198 @@
+/*
+ * ffbf.h -- C ABI of the B200 feed-forward Bloom filter (FFBF) matcher.
+ *
+ * Drop-in for the x86 rabin-karp path of efficient/ffbf. The reference's interface for that path is the
+ * C++ class Filter<H, LEN> (src/rabin-karp/ffbf.h:43-93) plus the `ffbf` CLI (src/rabin-karp/ffbf.cpp:529-601);
+ * every entry point below names the member or step it replaces. Differences that are part of the contract:
+ *
+ *  - The filter geometry (LEN, K, S, cache and external region sizes) is a runtime ffbf_params value
+ *    instead of compile-time macros (src/rabin-karp/Makefile.am:1-32, ffbf.cpp:55-83). The same values give
+ *    bit-identical filters and outputs.
+ *  - Errors are status codes, never exceptions. FilterError (ffbf.h:31-41) becomes a non-zero ffbf_status
+ *    and ffbf_last_error() holds its message.
+ *  - Inputs are byte buffers (a pattern file image, a text image) rather than file descriptors; the CLI
+ *    (ffbf_b200/csrc/ffbf_cli.cpp) and the C++ mirror (include/ffbf.hpp) read files and call these.
+ *  - All computation runs on one CUDA device. There is no CPU fallback: without a usable device,
+ *    ffbf_create fails with FFBF_ECUDA.
+ *
+ * Threading: one context is used by one host thread at a time. Distinct contexts are independent and may
+ * run concurrently on different streams. Result pointers returned in ffbf_*_result structs are owned by
+ * the context and stay valid until the next call of the same kind on that context, or ffbf_destroy.
+ */
+#ifndef FFBF_B200_FFBF_H
+#define FFBF_B200_FFBF_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+typedef enum {
+    FFBF_OK = 0,
+    FFBF_EINVAL = 1,          /* bad argument: geometry, NULL pointer, misaligned device pointer, bad file */
+    FFBF_ENOMEM_DEVICE = 2,   /* device allocation failed or would exceed the context's HBM budget */
+    FFBF_EIO = 3,             /* file open/read/write failed (the *_file entry points) */
+    FFBF_ETIMEOUT = 4,        /* a bounded device-side wait gave up (batched/served forms) */
+    FFBF_ECUDA = 5,           /* a CUDA runtime call failed; ffbf_last_error has the CUDA message */
+    FFBF_ESTATE = 6,          /* call out of order, e.g. ffbf_build before ffbf_set_patterns */
+    FFBF_ENOMEM_HOST = 7      /* host allocation failed */
+} ffbf_status;
+
+/* Filter geometry. Field <-> reference macro: len = DEF_PATT_LEN, k = DEF_K, s = DEF_S,
+ * cache_bits = DEF_CACHE_SIZE, ext_bits = DEF_EXT_SIZE (ffbf.cpp:55-77, 79-83).
+ * Constraints (those of the reference's uint32 arithmetic): 1 <= len <= 63, 1 <= k <= 11, 0 <= s <= k,
+ * cache_bits and ext_bits powers of two, cache_bits + ext_bits <= 2^31. */
+typedef struct {
+    uint32_t len;
+    uint32_t k;
+    uint32_t s;
+    uint32_t reserved;     /* must be 0 */
+    uint64_t cache_bits;
+    uint64_t ext_bits;
+} ffbf_params;
+
+typedef struct ffbf_ctx ffbf_ctx;
+
+/* Fills the reference's compile-time defaults: LEN 19, K 5, S 2, 2^24 cache bits, 2^28 external bits
+ * (ffbf.cpp:55-77). */
+ffbf_status ffbf_params_default(ffbf_params* p);
+
+/* Filter<H,LEN>::Filter() (ffbf.cpp:87-108): allocates the main and the feed-forward bit arrays, N/8 bytes
+ * each with N = cache_bits + ext_bits, zeroed, on `device`. */
+ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out);
+
+/* Filter<H,LEN>::~Filter() (ffbf.cpp:110-116). NULL is accepted. */
+void ffbf_destroy(ffbf_ctx* ctx);
+
+/* FilterError::what() (ffbf.h:37-40) of the last failing call on ctx ("" if none). */
+const char* ffbf_last_error(const ffbf_ctx* ctx);
+const char* ffbf_status_string(ffbf_status s);
+
+/* Limits the device memory this context may allocate (bytes; 0 = no limit beyond the device's). */
+ffbf_status ffbf_set_hbm_budget(ffbf_ctx* ctx, uint64_t bytes);
+
+/* Pattern file image, split into lines on '\n' exactly as main()'s getline loop (ffbf.cpp:556-558) and
+ * filterPhrases (ffbf.cpp:426-447) do: a final line without '\n' is a line; a trailing '\n' adds none.
+ * Copies the image to the device and hashes every line's LEN-byte prefix there. Sets no filter bits. */
+ffbf_status ffbf_set_patterns(ffbf_ctx* ctx, const uint8_t* file, size_t len);
+
+/* `filter << phrase` for every pattern line (operator<<, ffbf.cpp:268-283): lines shorter than LEN are
+ * skipped; otherwise K bits of the main filter are set in getHashValue order (ffbf.cpp:135-159). */
+ffbf_status ffbf_build(ffbf_ctx* ctx);
+
+/* ffbf_set_patterns followed by ffbf_build. */
+ffbf_status ffbf_add_patterns(ffbf_ctx* ctx, const uint8_t* file, size_t len);
+
+/* loadFilterFromFile (ffbf.cpp:487-506): ORs the bits of a __bloom_filter_* image (consecutive
+ * little-endian uint32 deltas between set-bit indices) into the main filter. A trailing partial word is
+ * ignored. An index at or beyond N gives FFBF_EINVAL and leaves the filter unchanged. */
+ffbf_status ffbf_load_filter(ffbf_ctx* ctx, const uint8_t* data, size_t len);
+
+/* saveFilterToFile (ffbf.cpp:508-527): encodes the main filter in the same delta format. *data is
+ * allocated by the library; release it with ffbf_free. */
+ffbf_status ffbf_save_filter(ffbf_ctx* ctx, uint8_t** data, size_t* len);
+
+/* File-path forms of the two above, for the CLI's __bloom_filter_<patterns> cache (ffbf.cpp:545-575). */
+ffbf_status ffbf_load_filter_file(ffbf_ctx* ctx, const char* path);
+ffbf_status ffbf_save_filter_file(ffbf_ctx* ctx, const char* path);
+
+/* Result of one scan. hit_offsets: start offset of every window whose K main bits are all set, ascending.
+ * line_start/line_end: the lines holding at least one such window, in text order; a line is
+ * [line_start, line_end) and excludes its '\n'. */
+typedef struct {
+    uint64_t text_len;
+    uint64_t n_hits;
+    const uint64_t* hit_offsets;
+    uint64_t n_lines;
+    const uint64_t* line_start;
+    const uint64_t* line_end;
+} ffbf_scan_result;
+
+/* processFile (ffbf.cpp:310-392) over a host text image: the hash rolls over every line ('\n' resets it
+ * and is not hashed); every window whose K main bits are set marks its line and sets K bits of the
+ * feed-forward filter in getHashValue_2 order (ffbf.cpp:161-185). The feed-forward filter accumulates
+ * over successive scans, as it does over one reference run; ffbf_clear_ff starts a new one. */
+ffbf_status ffbf_scan(ffbf_ctx* ctx, const uint8_t* text, size_t len, ffbf_scan_result* out);
+
+/* The same scan over a text already in device memory (16-byte aligned), enqueued on the context's
+ * stream; ffbf_scan_collect waits for it and fills `out`. */
+ffbf_status ffbf_scan_device(ffbf_ctx* ctx, const uint8_t* d_text, size_t len);
+ffbf_status ffbf_scan_collect(ffbf_ctx* ctx, ffbf_scan_result* out);
+
+/* What processFile writes to stdout for the last scan: every flagged line followed by '\n', with the
+ * reference's output rules reproduced byte for byte -- each line is printed as C strings (cut at its
+ * first NUL), and a line crossing read() chunk boundaries of `chunk` bytes (512 KiB in the reference,
+ * ffbf.cpp:313, when reading a regular file) prints only its last two chunks' parts (the carry buffer is
+ * overwritten, ffbf.cpp:372-382); a flagged final line without '\n' prints only its last chunk's part.
+ * Needs the host text image the scan ran on. *out is library-allocated; release with ffbf_free. */
+ffbf_status ffbf_format_lines(ffbf_ctx* ctx, const uint8_t* text, size_t len, size_t chunk,
+                              uint8_t** out, size_t* out_len);
+
+/* The output rule above as a stand-alone host function: writes buf[start[i], end[i]) for each i, each
+ * followed by '\n', exactly as processFile/filterPhrases print a flagged line of a `len`-byte input read in
+ * `chunk`-byte pieces (C-string cut at NUL; carry of the previous chunk only; a final line without '\n'
+ * prints only its last chunk's part). end[i] == len marks a final line without '\n'. Spans must be
+ * ascending, non-overlapping lines of buf. Needs no context and no device. Library-allocated output. */
+ffbf_status ffbf_format_spans(const uint8_t* buf, size_t len, const uint64_t* start, const uint64_t* end, size_t n,
+                              size_t chunk, uint8_t** out, size_t* out_len);
+
+/* Result of the feed-forward pass: 0-based line numbers of the surviving patterns, ascending. */
+typedef struct {
+    uint64_t n_ids;
+    const uint64_t* ids;
+} ffbf_prune_result;
+
+/* filterPhrases (ffbf.cpp:394-485): a pattern line survives when it is at least LEN bytes long and its
+ * prefix window has all K feed-forward bits set (getHashValue_2 order). */
+ffbf_status ffbf_prune(ffbf_ctx* ctx, ffbf_prune_result* out);
+
+/* The two files filterPhrases writes for the last prune: the pruned pattern file (each surviving line
+ * then '\n', with the C-string and chunk-carry rules of ffbf.cpp:431-442,464-481 over `chunk`-byte reads of
+ * the pattern file) and the __index_ file (one decimal line number per line). Library-allocated. */
+ffbf_status ffbf_format_pruned(ffbf_ctx* ctx, size_t chunk, uint8_t** out, size_t* out_len,
+                               uint8_t** index, size_t* index_len);
+
+/* Exact matches: every (offset, pattern line number) where a pruned pattern's full bytes occur in the
+ * last scanned text at a hit window's start. This is the `grep -Ff pruned candidates` step of the
+ * reference workflow (src/rabin-karp/README:49-52) done on the device: candidates are looked up by their
+ * 64-bit window hash in a table of the pruned patterns' prefix hashes, then byte-compared.
+ * Sorted by offset, then pattern id. Patterns shorter than LEN are never reported (ffbf.cpp:271-275). */
+typedef struct {
+    uint64_t n;
+    const uint64_t* offsets;
+    const uint64_t* pattern_ids;
+} ffbf_matches;
+ffbf_status ffbf_verify(ffbf_ctx* ctx, ffbf_matches* out);
+
+/* operator[] (ffbf.cpp:285-308): 1 when some LEN-byte window of `line` has all K main bits set. Like the
+ * reference, '\n' inside `line` is hashed as an ordinary byte, and lines shorter than LEN give 0. */
+ffbf_status ffbf_test_line(ffbf_ctx* ctx, const uint8_t* line, size_t len, int* hit);
+
+/* Zeroes the feed-forward filter (a fresh reverseBitvector, ffbf.cpp:107). Enqueued on the context's
+ * stream; later calls on the context see it done. */
+ffbf_status ffbf_clear_ff(ffbf_ctx* ctx);
+
+/* Copies the main and/or feed-forward bit arrays (N/8 bytes each, bit i = byte i>>3, mask 1<<(i&7), as
+ * setBit at ffbf.cpp:187-193) to host memory. Either pointer may be NULL. */
+ffbf_status ffbf_get_filters(ffbf_ctx* ctx, uint8_t* main_bits, uint8_t* ff_bits);
+
+/* Size in bytes of one bit array (N/8). */
+uint64_t ffbf_filter_bytes(const ffbf_ctx* ctx);
+
+/* The context's CUDA stream (a cudaStream_t). Every device operation of the context is ordered on it;
+ * callers may record events on it or make other streams wait on it. */
+void* ffbf_stream(ffbf_ctx* ctx);
+
+/* Number of CUDA kernels this library has launched in the process so far (all contexts). */
+uint64_t ffbf_kernel_launches(void);
+
+/* Releases memory the library allocated for an out-parameter. */
+void ffbf_free(void* p);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* FFBF_B200_FFBF_H */

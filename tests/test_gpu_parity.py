@@ -1,0 +1,173 @@
+"""Parity of the CUDA path (through the C ABI) with the reference binary's outputs and the oracle.
+
+Each golden case runs: filter build on the device -> __bloom_filter_ image; scan -> stdout bytes, hit
+offsets, line spans, feed-forward bit array; prune -> pruned file + __index_ file; verification -> exact
+(offset, pattern id) pairs. All comparisons are bit-exact.
+"""
+import os
+import subprocess
+import tempfile
+
+import numpy as np
+import pytest
+
+import oracle
+from cases import CASES, build_inputs
+from conftest import ROOT, Golden
+from ffbf_b200 import FFBFError, Filter, Params
+
+pytestmark = pytest.mark.gpu
+
+
+def delta(bits):
+    return np.diff(np.concatenate([[0], np.asarray(bits, dtype=np.uint64)])).astype("<u4").tobytes()
+
+
+@pytest.fixture(scope="module", autouse=True)
+def require_gpu():
+    import torch
+    assert torch.cuda.is_available(), "the gpu tests need a CUDA device"
+
+
+def run_oracle(prm, pats, text):
+    o = oracle.Oracle.from_params(prm)
+    o.build(pats)
+    s = o.scan(text)
+    pr = o.prune(pats)
+    off, pid = o.verify(pats, pr["ids"], text, s["hits"])
+    return o, s, pr, off, pid
+
+
+@pytest.mark.parametrize("name", list(CASES))
+def test_parity_with_reference_and_oracle(name):
+    g = Golden(name)
+    prm, pats, text = build_inputs(name)
+    o, s, pr, ooff, opid = run_oracle(prm, pats, text)
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        assert g.matches("bloom", f.save_filter())
+        r = f.process(text)
+        np.testing.assert_array_equal(r.hit_offsets, s["hits"])
+        np.testing.assert_array_equal(r.line_start, s["line_start"])
+        np.testing.assert_array_equal(r.line_end, s["line_end"])
+        assert g.matches("stdout", f.format_lines(text))
+        main, ff = f.get_filters()
+        assert np.array_equal(main, o.main)
+        assert np.array_equal(ff, o.ff)
+        assert g.matches("ff", delta(oracle.set_bits(ff)))
+        ids = f.filter_phrases()
+        np.testing.assert_array_equal(ids, pr["ids"])
+        out, idx = f.format_pruned()
+        assert g.matches("pruned", out) and g.matches("index", idx)
+        off, pid = f.verify()
+        np.testing.assert_array_equal(off, ooff)
+        np.testing.assert_array_equal(pid, opid)
+
+
+@pytest.mark.parametrize("name", ["plain_small", "scale_small", "edge_mixed"])
+def test_loaded_filter_gives_same_results(name):
+    """The CLI's cached-filter path: patterns set without building, main filter from the bloom file."""
+    g = Golden(name)
+    prm, pats, text = build_inputs(name)
+    o, s, pr, _, _ = run_oracle(prm, pats, text)
+    with Filter(prm) as f:
+        f.set_patterns(pats)
+        f.load_filter(o.save_filter())
+        r = f.process(text)
+        np.testing.assert_array_equal(r.hit_offsets, s["hits"])
+        assert g.matches("stdout", f.format_lines(text))
+        np.testing.assert_array_equal(f.filter_phrases(), pr["ids"])
+
+
+def test_device_resident_text_matches_host_text():
+    import torch
+    prm, pats, text = build_inputs("scale_small")
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        host = f.process(text)
+        f.clear_ff()
+        dt = torch.from_numpy(text).cuda()
+        f.process_device(dt.data_ptr(), text.size)
+        dev = f.collect()
+        np.testing.assert_array_equal(host.hit_offsets, dev.hit_offsets)
+        np.testing.assert_array_equal(host.line_start, dev.line_start)
+
+
+def test_feed_forward_accumulates_over_scans():
+    prm, pats, text = build_inputs("plain_small")
+    o, s, pr, _, _ = run_oracle(prm, pats, text)
+    cut = int(np.flatnonzero(text[: text.size // 2] == 10)[-1]) + 1
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        a = f.process(text[:cut])
+        b = f.process(text[cut:])
+        hits = np.concatenate([a.hit_offsets, b.hit_offsets + cut])
+        np.testing.assert_array_equal(hits, s["hits"])
+        np.testing.assert_array_equal(f.get_filters()[1], o.ff)
+        np.testing.assert_array_equal(f.filter_phrases(), pr["ids"])
+
+
+def test_hit_buffer_regrows():
+    prm, pats, text = build_inputs("hit_flood")
+    o, s, _, _, _ = run_oracle(prm, pats, text)
+    assert s["hits"].size > 65536, "case must overflow the initial hit buffer"
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        np.testing.assert_array_equal(f.process(text).hit_offsets, s["hits"])
+
+
+def test_test_line_matches_oracle():
+    prm, pats, text = build_inputs("dense_fp")
+    o = oracle.Oracle.from_params(prm)
+    o.build(pats)
+    lines = bytes(text[:200_000]).split(b"\n")[:400] + [pats.split(b"\n")[0], b"", b"x" * 19, b"a\nb" * 20]
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        for ln in lines:
+            assert f.test_line(ln) == o.test_line(ln), ln
+
+
+def test_hbm_budget_is_enforced():
+    prm, pats, text = build_inputs("plain_small")
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        f.set_hbm_budget(1)
+        with pytest.raises(FFBFError) as e:
+            f.process(text)
+        assert e.value.status == 2
+
+
+def test_bad_filter_file_rejected():
+    prm = Params(20, 5, 2, 1 << 12, 1 << 14)
+    with Filter(prm) as f:
+        bad = np.array([5, prm.nbits], dtype="<u4").tobytes()
+        with pytest.raises(FFBFError) as e:
+            f.load_filter(bad)
+        assert e.value.status == 1
+        assert not f.get_filters()[0].any()
+
+
+def test_cli_matches_reference_files():
+    g = Golden("plain_small")
+    prm, pats, text = build_inputs("plain_small")
+    cli = os.path.join(ROOT, "ffbf_b200", "_lib", "ffbf")
+    with tempfile.TemporaryDirectory() as wd:
+        open(os.path.join(wd, "pats"), "wb").write(pats)
+        open(os.path.join(wd, "text"), "wb").write(text.tobytes())
+        for run in range(2):  # the second run loads __bloom_filter_pats
+            with open(os.path.join(wd, "text"), "rb") as fin:
+                r = subprocess.run([cli, "--len", "20", "pats", "out"], stdin=fin, capture_output=True, cwd=wd)
+            assert r.returncode == 0, r.stderr
+            assert g.matches("stdout", r.stdout)
+            assert g.matches("pruned", open(os.path.join(wd, "out"), "rb").read())
+            assert g.matches("index", open(os.path.join(wd, "__index_out"), "rb").read())
+            assert g.matches("bloom", open(os.path.join(wd, "__bloom_filter_pats"), "rb").read())
+            assert (b"filter load time:" in r.stderr) == (run == 1)
+            assert b"processFile time:" in r.stderr and b"filterPhrases time:" in r.stderr
+        with open(os.path.join(wd, "text"), "rb") as fin:
+            r = subprocess.run([cli, "--len", "20", "--exact", "pats", "out"], stdin=fin, capture_output=True, cwd=wd)
+        assert r.returncode == 0
+        # --exact prints the lines `grep -F -f pats` prints (all patterns here are >= LEN bytes)
+        g = subprocess.run(["grep", "-F", "-a", "-f", "pats", "text"], capture_output=True, cwd=wd,
+                           env=dict(os.environ, LC_ALL="C"))
+        assert r.stdout == g.stdout and len(g.stdout) > 0

@@ -1,0 +1,96 @@
+"""Host-side checks that need no GPU: the C ABI's exports, argument validation, and the output formatting
+rules (ffbf_format_spans) against the oracle's literal restatement of processFile."""
+import ctypes
+import os
+import re
+import subprocess
+
+import numpy as np
+import pytest
+
+import ffbf_b200
+import oracle
+from cases import build_inputs
+from conftest import ROOT, has_gpu
+
+
+def header_functions():
+    src = open(os.path.join(ROOT, "include", "ffbf.h")).read()
+    return sorted(set(re.findall(r"\b(ffbf_[a-z_0-9]+)\s*\(", src)))
+
+
+def test_library_exports_every_declared_function():
+    lib = ffbf_b200.load_library()
+    names = header_functions()
+    assert len(names) >= 26
+    for n in names:
+        assert hasattr(lib, n), f"{n} declared in include/ffbf.h but not exported"
+    assert set(ffbf_b200.EXPORTED) >= set(names)
+    out = subprocess.run(["nm", "-D", "--defined-only", ffbf_b200.lib.LIB_PATH], capture_output=True, text=True).stdout
+    exported = set(re.findall(r" T (ffbf_[a-z_0-9]+)$", out, re.M))
+    assert set(names) <= exported
+
+
+def test_status_strings_and_defaults():
+    lib = ffbf_b200.load_library()
+    assert lib.ffbf_status_string(0) == b"ok"
+    assert lib.ffbf_status_string(5) == b"CUDA error"
+    p = ffbf_b200.Params(1, 1, 1, 32, 32)
+    assert lib.ffbf_params_default(ctypes.byref(p)) == 0
+    assert p.as_tuple() == (19, 5, 2, 1 << 24, 1 << 28)
+
+
+@pytest.mark.parametrize("bad", [
+    (0, 5, 2, 1 << 24, 1 << 28), (64, 5, 2, 1 << 24, 1 << 28), (19, 0, 0, 1 << 24, 1 << 28),
+    (19, 12, 2, 1 << 24, 1 << 28), (19, 5, 6, 1 << 24, 1 << 28), (19, 5, 2, 3 << 20, 1 << 28),
+    (19, 5, 2, 16, 1 << 28), (19, 5, 2, 1 << 31, 1 << 31)])
+def test_create_rejects_bad_geometry(bad):
+    lib = ffbf_b200.load_library()
+    h = ctypes.c_void_p()
+    assert lib.ffbf_create(ctypes.byref(ffbf_b200.Params(*bad)), 0, ctypes.byref(h)) == 1
+    assert not h.value
+
+
+@pytest.mark.skipif(has_gpu(), reason="a GPU is present")
+def test_create_without_gpu_fails_loudly():
+    with pytest.raises(ffbf_b200.FFBFError) as e:
+        ffbf_b200.Filter(ffbf_b200.Params())
+    assert e.value.status == 5
+
+
+@pytest.mark.parametrize("name", ["edge_chunks", "edge_nul_chunk", "edge_mixed", "plain_small", "binary_small"])
+@pytest.mark.parametrize("chunk", [512 * 1024, 4096, 97])
+def test_format_spans_matches_processfile_output(name, chunk):
+    prm, pats, text = build_inputs(name)
+    o = oracle.Oracle.from_params(prm)
+    o.build(pats)
+    s = o.scan(text, chunk=chunk)
+    assert ffbf_b200.format_spans(text, s["line_start"], s["line_end"], chunk) == s["out"]
+
+
+@pytest.mark.parametrize("chunk", [512 * 1024, 1000])
+def test_format_spans_matches_filterphrases_output(chunk):
+    prm, pats, text = build_inputs("dense_fp")
+    o = oracle.Oracle.from_params(prm)
+    o.build(pats)
+    o.scan(text)
+    pr = o.prune(pats, chunk=chunk)
+    pa = np.frombuffer(pats, np.uint8)
+    nl = np.flatnonzero(pa == 10)
+    starts = np.concatenate([[0], nl + 1])[pr["ids"].astype(np.int64)]
+    ends = np.concatenate([nl, [pa.size]])[pr["ids"].astype(np.int64)]
+    assert ffbf_b200.format_spans(pats, starts, ends, chunk) == pr["out"]
+
+
+def test_format_spans_rejects_bad_spans():
+    with pytest.raises(ffbf_b200.FFBFError):
+        ffbf_b200.format_spans(b"abc\ndef\n", [4, 0], [7, 3])
+    with pytest.raises(ffbf_b200.FFBFError):
+        ffbf_b200.format_spans(b"abc\n", [0], [9])
+
+
+def test_cli_usage_error():
+    cli = os.path.join(ROOT, "ffbf_b200", "_lib", "ffbf")
+    r = subprocess.run([cli, "only_one_arg"], capture_output=True)
+    assert r.returncode == 255
+    assert b"Usage: ffbf phrases phrases.out < corpus > filtered_corpus" in r.stderr
