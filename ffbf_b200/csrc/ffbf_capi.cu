@@ -61,6 +61,9 @@ struct ffbf_ctx {
     long long* d_tiles = nullptr;  // 4 arrays of tiles_cap: first, last, prev, next
     uint64_t tiles_cap = 0;
     int scan_path = 0;             // 0 = generic, 1 = fast
+    uint32_t* d_stage1 = nullptr;  // stage-1 table of the tuned scan (cache copy or summary)
+    bool stage1_dirty = true;
+    bool force_generic = false;    // FFBF_FORCE_GENERIC_SCAN=1 in the environment
     std::vector<uint64_t> r_hits, r_ls, r_le;
 
     // prune
@@ -256,9 +259,14 @@ ffbf_status launch_scan(ffbf_ctx* c) {
     a.tile_first_nl = c->d_tiles;
     a.tile_last_nl = c->d_tiles + c->tiles_cap;
     a.ntiles = ntiles;
-    if (ffbf::fast_scan_supported(c->g, n)) {
+    if (ffbf::fast_scan_supported(c->g, n) && !c->force_generic) {
         c->scan_path = 1;
-        CUDA_TRY(c, ffbf::scan_fast(a, c->num_sms, c->st));
+        if (!c->d_stage1) TRY(dalloc_t(c, &c->d_stage1, ffbf::stage1_words_for(c->g)));
+        if (c->stage1_dirty) {
+            CUDA_TRY(c, ffbf::build_stage1(c->d_main, c->g, c->d_stage1, c->st));
+            c->stage1_dirty = false;
+        }
+        CUDA_TRY(c, ffbf::scan_fast(a, c->d_stage1, c->num_sms, c->st));
     } else {
         c->scan_path = 0;
         a.cache_in_smem = c->g.cache_bits <= ffbf::kSmemCacheMaxBits;
@@ -348,6 +356,8 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
         cudaGetLastError();
         return bail(FFBF_ECUDA);
     }
+    const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");
+    c->force_generic = fg && fg[0] == '1';
     *out = c;
     return FFBF_OK;
 }
@@ -435,6 +445,7 @@ ffbf_status ffbf_build(ffbf_ctx* c) {
     TRY(enter(c));
     if (!c->have_patterns) return fail(c, FFBF_ESTATE, "ffbf_build needs ffbf_set_patterns first");
     CUDA_TRY(c, ffbf::hash_patterns(c->d_pat, c->d_pstart, c->d_pend, c->npat, c->g, c->d_phash, c->d_main, 1, c->st));
+    c->stage1_dirty = true;
     return sync(c);
 }
 
@@ -462,7 +473,7 @@ ffbf_status ffbf_load_filter(ffbf_ctx* c, const uint8_t* data, size_t len) {
             s = fail(c, FFBF_ECUDA, "filter decode failed: %s", cudaGetErrorString(cudaGetLastError()));
         } else if (err) {
             s = fail(c, FFBF_EINVAL, "filter file holds a bit index at or beyond N = %u", c->g.nbits);
-        } else if (ffbf::filter_set_indices(d_idx, nd, c->d_main, c->st) != cudaSuccess ||
+        } else if ((c->stage1_dirty = true, ffbf::filter_set_indices(d_idx, nd, c->d_main, c->st) != cudaSuccess) ||
                    cudaStreamSynchronize(c->st) != cudaSuccess) {
             s = fail(c, FFBF_ECUDA, "filter load failed: %s", cudaGetErrorString(cudaGetLastError()));
         }

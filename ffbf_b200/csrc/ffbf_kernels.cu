@@ -223,7 +223,7 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_generic(ScanArgs a) {
         for (uint32_t w = tid; w < g.cache_bits / 32; w += kScanThreads) s_cache[w] = a.main_words[w];
     const uint32_t* cache_words = a.cache_in_smem ? s_cache : a.main_words;
 
-    for (uint64_t tile = blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
+    for (uint64_t tile = a.tile_begin + blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
         __syncthreads();
         const long long t0 = (long long)(tile * kScanTile);
         for (int q = tid; q < (kScanTile + kHalo) / 4; q += kScanThreads) {
@@ -310,7 +310,7 @@ cudaError_t scan_generic(const ScanArgs& a, int grid, cudaStream_t st) {
     size_t smem = scan_smem_bytes(a.cache_in_smem, a.g);
     cudaError_t e = cudaFuncSetAttribute(k_scan_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    if (a.ntiles == 0) return cudaSuccess;
+    if (a.ntiles <= a.tile_begin) return cudaSuccess;
     k_scan_generic<<<grid, kScanThreads, smem, st>>>(a);
     note_launches(1);
     return cudaGetLastError();

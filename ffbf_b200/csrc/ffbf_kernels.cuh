@@ -46,6 +46,7 @@ struct ScanArgs {
     long long* tile_first_nl;  // per tile: first '\n' position in the tile, or LLONG_MAX
     long long* tile_last_nl;   // per tile: last '\n' position in the tile, or -1
     uint64_t ntiles;
+    uint64_t tile_begin;  // first tile this launch handles (tiles before it belong to another kernel)
     int cache_in_smem;
 };
 

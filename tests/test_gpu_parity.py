@@ -171,3 +171,18 @@ def test_cli_matches_reference_files():
         g = subprocess.run(["grep", "-F", "-a", "-f", "pats", "text"], capture_output=True, cwd=wd,
                            env=dict(os.environ, LC_ALL="C"))
         assert r.stdout == g.stdout and len(g.stdout) > 0
+
+
+@pytest.mark.parametrize("name", ["plain_small", "scale_small", "smem_cache", "edge_chunks", "binary_small"])
+def test_generic_and_tuned_scans_agree(name, monkeypatch):
+    """The generic kernel (any geometry) and the tuned sm_100a kernel give identical results."""
+    prm, pats, text = build_inputs(name)
+    outs = []
+    for force in ("1", "0"):
+        monkeypatch.setenv("FFBF_FORCE_GENERIC_SCAN", force)
+        with Filter(prm) as f:
+            f.add_patterns(pats)
+            r = f.process(text)
+            outs.append((r.hit_offsets, r.line_start, r.line_end, f.get_filters()[1]))
+    for a, b in zip(*outs):
+        np.testing.assert_array_equal(a, b)
