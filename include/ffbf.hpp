@@ -1,0 +1,166 @@
+// ffbf.hpp -- C++ mirror of efficient/ffbf's Filter<H, LEN> (src/rabin-karp/ffbf.h:43-93) over the C ABI.
+//
+// A program written against the reference class switches by replacing
+//     #include "ffbf.h"                                   (src/rabin-karp/ffbf.h)
+//     Filter<hash_rot_sbox_pre_2<DEF_PATT_LEN>, DEF_PATT_LEN> filter;
+// with
+//     #include "ffbf.hpp"                                 (this file; link with -lffbf)
+//     ffbf::Filter filter;                                (or ffbf::Filter filter(params, device))
+// and keeps its calls: `filter << phrase`, `filter[line]`, processFile(fd), filterPhrases(pfd, out, outIndex),
+// loadFilterFromFile(fd), saveFilterToFile(fd). Errors are thrown as FilterError (ffbf.h:31-41), whose what()
+// carries the library's message. The geometry defaults to the reference's compile-time defaults.
+//
+// Differences, all documented in include/ffbf.h: the filter lives on a CUDA device; `filter << phrase` buffers
+// patterns and the device build runs once, before the first operation that needs the filter; processFile
+// reads the whole stream before scanning it.
+#ifndef FFBF_B200_FFBF_HPP
+#define FFBF_B200_FFBF_HPP
+
+#include <unistd.h>
+
+#include <fstream>
+#include <string>
+#include <vector>
+
+#include "ffbf.h"
+
+namespace ffbf {
+
+class FilterError {
+    std::string message;
+
+public:
+    explicit FilterError(const std::string& msg = "") : message(msg) {}
+    const char* what() const { return message.c_str(); }
+};
+
+class Filter {
+public:
+    explicit Filter(const ffbf_params* p = nullptr, int device = 0) {
+        ffbf_params d;
+        ffbf_params_default(&d);
+        ffbf_status s = ffbf_create(p ? p : &d, device, &ctx_);
+        if (s != FFBF_OK) throw FilterError(std::string("Not able to initialize filter: ") + ffbf_status_string(s));
+    }
+    ~Filter() { ffbf_destroy(ctx_); }
+    Filter(const Filter&) = delete;
+    Filter& operator=(const Filter&) = delete;
+
+    // operator<< (ffbf.cpp:268-283): queue one pattern line; lines shorter than LEN are ignored at build time.
+    Filter& operator<<(const std::string& pattern) {
+        pending_.insert(pending_.end(), pattern.begin(), pattern.end());
+        pending_.push_back('\n');
+        dirty_ = true;
+        return *this;
+    }
+
+    // operator[] (ffbf.cpp:285-308): does some window of `line` hit the main filter?
+    bool operator[](const std::string& line) {
+        flush();
+        int hit = 0;
+        check(ffbf_test_line(ctx_, reinterpret_cast<const uint8_t*>(line.data()), line.size(), &hit));
+        return hit != 0;
+    }
+
+    // processFile (ffbf.cpp:310-392): reads fd to its end, scans it, writes the candidate lines to stdout
+    // with the reference's output rules (512 KiB read() chunks of a regular file).
+    void processFile(int fd) {
+        flush();
+        std::vector<uint8_t> text;
+        std::vector<uint8_t> buf(1 << 20);
+        for (;;) {
+            ssize_t r = ::read(fd, buf.data(), buf.size());
+            if (r < 0) throw FilterError("Error while reading from file");
+            if (r == 0) break;
+            text.insert(text.end(), buf.begin(), buf.begin() + r);
+        }
+        ffbf_scan_result res;
+        check(ffbf_scan(ctx_, text.data(), text.size(), &res));
+        uint8_t* out = nullptr;
+        size_t n = 0;
+        check(ffbf_format_lines(ctx_, text.data(), text.size(), 512 * 1024, &out, &n));
+        size_t off = 0;
+        while (off < n) {
+            ssize_t w = ::write(1, out + off, n - off);
+            if (w <= 0) break;
+            off += (size_t)w;
+        }
+        ffbf_free(out);
+    }
+
+    // filterPhrases (ffbf.cpp:394-485): re-reads the pattern file from pfd, writes the surviving lines to
+    // `out` and their 0-based line numbers to `outIndex`.
+    void filterPhrases(int pfd, std::ofstream& out, std::ofstream& outIndex) {
+        flush();
+        std::vector<uint8_t> pats;
+        std::vector<uint8_t> buf(1 << 20);
+        for (;;) {
+            ssize_t r = ::read(pfd, buf.data(), buf.size());
+            if (r < 0) throw FilterError("Error while reading from file");
+            if (r == 0) break;
+            pats.insert(pats.end(), buf.begin(), buf.begin() + r);
+        }
+        check(ffbf_set_patterns(ctx_, pats.data(), pats.size()));
+        ffbf_prune_result pr;
+        check(ffbf_prune(ctx_, &pr));
+        uint8_t *o = nullptr, *ix = nullptr;
+        size_t on = 0, in = 0;
+        check(ffbf_format_pruned(ctx_, 512 * 1024, &o, &on, &ix, &in));
+        out.write(reinterpret_cast<const char*>(o), (std::streamsize)on);
+        outIndex.write(reinterpret_cast<const char*>(ix), (std::streamsize)in);
+        ffbf_free(o);
+        ffbf_free(ix);
+    }
+
+    // loadFilterFromFile / saveFilterToFile (ffbf.cpp:487-527): the __bloom_filter_ delta format.
+    void loadFilterFromFile(int fd) {
+        std::vector<uint8_t> data;
+        std::vector<uint8_t> buf(1 << 20);
+        for (;;) {
+            ssize_t r = ::read(fd, buf.data(), buf.size());
+            if (r < 0) throw FilterError("Error while reading from the filter file");
+            if (r == 0) break;
+            data.insert(data.end(), buf.begin(), buf.begin() + r);
+        }
+        check(ffbf_load_filter(ctx_, data.data(), data.size()));
+    }
+
+    void saveFilterToFile(int fd) {
+        flush();
+        uint8_t* data = nullptr;
+        size_t n = 0;
+        check(ffbf_save_filter(ctx_, &data, &n));
+        size_t off = 0;
+        while (off < n) {
+            ssize_t w = ::write(fd, data + off, n - off);
+            if (w < 0) {
+                ffbf_free(data);
+                throw FilterError("Error while writing to the filter file");
+            }
+            off += (size_t)w;
+        }
+        ffbf_free(data);
+    }
+
+    ffbf_ctx* handle() { return ctx_; }
+
+private:
+    void check(ffbf_status s) {
+        if (s != FFBF_OK) throw FilterError(std::string(ffbf_status_string(s)) + ": " + ffbf_last_error(ctx_));
+    }
+    // Builds the queued patterns into the main filter (the reference sets bits inside operator<<).
+    void flush() {
+        if (!dirty_) return;
+        check(ffbf_set_patterns(ctx_, pending_.data(), pending_.size()));
+        check(ffbf_build(ctx_));
+        dirty_ = false;
+    }
+
+    ffbf_ctx* ctx_ = nullptr;
+    std::vector<uint8_t> pending_;
+    bool dirty_ = false;
+};
+
+}  // namespace ffbf
+
+#endif  // FFBF_B200_FFBF_HPP
