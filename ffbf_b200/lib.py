@@ -35,7 +35,7 @@ EXPORTED = [
     "ffbf_save_filter", "ffbf_load_filter_file", "ffbf_save_filter_file", "ffbf_scan", "ffbf_scan_device",
     "ffbf_scan_collect", "ffbf_format_lines", "ffbf_prune", "ffbf_format_pruned", "ffbf_verify",
     "ffbf_test_line", "ffbf_clear_ff", "ffbf_get_filters", "ffbf_filter_bytes", "ffbf_free", "ffbf_format_spans",
-    "ffbf_stream", "ffbf_kernel_launches",
+    "ffbf_stream", "ffbf_kernel_launches", "ffbf_scan_static",
 ]
 
 
@@ -122,6 +122,8 @@ def load_library(path=LIB_PATH):
         "ffbf_format_spans": (ctypes.c_int, [vp, sz, vp, vp, sz, sz, P(u8p), P(sz)]),
         "ffbf_stream": (vp, [vp]),
         "ffbf_kernel_launches": (ctypes.c_uint64, []),
+        "ffbf_scan_static": (ctypes.c_int, [P(Params), vp, vp, vp, ctypes.c_uint64, vp, vp, vp,
+                                            P(ctypes.c_uint32), vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)

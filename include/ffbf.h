@@ -188,6 +188,29 @@ void* ffbf_stream(ffbf_ctx* ctx);
 /* Number of CUDA kernels this library has launched in the process so far (all contexts). */
 uint64_t ffbf_kernel_launches(void);
 
+/* ffbf_scan_static: processFile's scan, run without allocating any device or host memory. This entry
+ * point has no counterpart in the reference; it exists for callers that may not call cudaMalloc -- a
+ * program whose own allocator owns every byte of device memory, a plug-in host that forbids allocation
+ * in callbacks, a latency-critical loop that cannot take an allocation's implicit synchronisation.
+ *
+ * The caller passes the geometry, the main filter d_main (N/8 bytes, the layout ffbf_get_filters
+ * returns), a feed-forward filter d_ff to OR hits into, the text (device, 16-byte aligned, at most
+ * FFBF_STATIC_MAX_TEXT bytes) and three device output arrays of FFBF_STATIC_MAX_HITS entries each. On
+ * return *n_hits holds the number of hit windows; d_hit_offsets[i] is a window start and
+ * [d_line_start[i], d_line_end[i]) its line, in no particular order. All scratch memory comes from one
+ * fixed device array of FFBF_STATIC_SCRATCH_BYTES compiled into the library, which every GPU that loads
+ * the library holds until the process exits. The first call on a device looks up that array's address
+ * for the device that is current. Work is ordered on `stream` (a cudaStream_t, 0 for the default);
+ * the call waits for it. Calls whose work overlaps on the GPU share the array and race: serialise them.
+ * Returns FFBF_EINVAL for a text longer than FFBF_STATIC_MAX_TEXT, and FFBF_ENOMEM_DEVICE when more than
+ * FFBF_STATIC_MAX_HITS windows hit (*n_hits then holds the full count, the arrays a subset of it). */
+#define FFBF_STATIC_MAX_TEXT (1ull << 30)
+#define FFBF_STATIC_MAX_HITS (1u << 16)
+#define FFBF_STATIC_SCRATCH_BYTES (256ull + 32ull * FFBF_STATIC_MAX_HITS + 32ull * (FFBF_STATIC_MAX_TEXT / 16384ull))
+ffbf_status ffbf_scan_static(const ffbf_params* p, const uint32_t* d_main, uint32_t* d_ff, const uint8_t* d_text,
+                             uint64_t len, uint64_t* d_hit_offsets, uint64_t* d_line_start, uint64_t* d_line_end,
+                             uint32_t* n_hits, void* stream);
+
 /* Releases memory the library allocated for an out-parameter. */
 void ffbf_free(void* p);
 
