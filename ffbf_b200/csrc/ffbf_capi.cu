@@ -63,6 +63,11 @@ struct ffbf_ctx {
     int scan_path = 0;             // 0 = generic, 1 = fast
     uint32_t* d_stage1 = nullptr;  // stage-1 table of the tuned scan (cache copy or summary)
     bool stage1_dirty = true;
+    uint32_t stage1_sh = 0;
+    unsigned long long* d_popc = nullptr;
+    double stage1_fill = 0;
+    int scan_mode = 0;             // 0 sparse, 1 dense (see ffbf_scan_fast.cu)
+    int force_mode = -1;           // FFBF_SCAN_MODE=0|1 in the environment
     bool force_generic = false;    // FFBF_FORCE_GENERIC_SCAN=1 in the environment
     std::vector<uint64_t> r_hits, r_ls, r_le;
 
@@ -261,12 +266,32 @@ ffbf_status launch_scan(ffbf_ctx* c) {
     a.ntiles = ntiles;
     if (ffbf::fast_scan_supported(c->g, n) && !c->force_generic) {
         c->scan_path = 1;
-        if (!c->d_stage1) TRY(dalloc_t(c, &c->d_stage1, ffbf::stage1_words_for(c->g)));
+        const uint32_t sh = ffbf::stage1_shift_for(c->g);
+        if (c->d_stage1 && c->stage1_sh != sh) {  // the CTA shape changed the table size
+            dfree(c, c->d_stage1);
+            c->stage1_dirty = true;
+        }
+        if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 1));
+        if (!c->d_stage1) {
+            TRY(dalloc_t(c, &c->d_stage1, ffbf::stage1_words_for(c->g)));
+            c->stage1_sh = sh;
+            c->stage1_dirty = true;
+        }
         if (c->stage1_dirty) {
             CUDA_TRY(c, ffbf::build_stage1(c->d_main, c->g, c->d_stage1, c->st));
+            // Mode choice: the shared-memory stage only pays while it rejects most windows.
+            const uint32_t nw = ffbf::stage1_words_for(c->g);
+            CUDA_TRY(c, ffbf::popcount_words(c->d_stage1, nw, c->d_popc, c->st));
+            unsigned long long ones = 0;
+            CUDA_TRY(c, cudaMemcpyAsync(&ones, c->d_popc, sizeof ones, cudaMemcpyDeviceToHost, c->st));
+            TRY(sync(c));
+            c->stage1_fill = (double)ones / (32.0 * nw);
+            c->scan_mode = c->stage1_fill > 0.3 ? 1 : 0;
             c->stage1_dirty = false;
         }
-        CUDA_TRY(c, ffbf::scan_fast(a, c->d_stage1, c->num_sms, c->st));
+        int mode = c->scan_mode;
+        if (c->force_mode >= 0) mode = c->force_mode;
+        CUDA_TRY(c, ffbf::scan_fast(a, c->d_stage1, mode, c->num_sms, c->st));
     } else {
         c->scan_path = 0;
         a.cache_in_smem = c->g.cache_bits <= ffbf::kSmemCacheMaxBits;
@@ -356,6 +381,10 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
         cudaGetLastError();
         return bail(FFBF_ECUDA);
     }
+    const char* th = getenv("FFBF_SCAN_THREADS");
+    if (th) ffbf::set_fast_scan_threads(atoi(th));
+    const char* fm = getenv("FFBF_SCAN_MODE");
+    if (fm && (fm[0] == '0' || fm[0] == '1')) c->force_mode = fm[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");
     c->force_generic = fg && fg[0] == '1';
     *out = c;

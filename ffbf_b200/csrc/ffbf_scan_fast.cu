@@ -5,24 +5,26 @@
 // row. Each thread rolls the hash over its stream without restarting, so the LEN-byte warm-up is paid once
 // per stream (from a 32-byte halo) instead of once per tile.
 //
-// Staging. Row r of all THREADS streams is one TMA load of a 3-D box {128 bytes, 1 row, THREADS streams}
-// (cp.async.bulk.tensor, 128B swizzle, no multicast) into a double-buffered shared-memory stage, completed on
-// an mbarrier. The 128B swizzle puts chunk c of thread t's row at chunk c ^ (t & 7), so the eight 16-byte
-// reads a quarter-warp issues hit eight different bank groups.
+// Staging. Row r of the CTA's streams is loaded by TMA as 3-D boxes {128 bytes, 1 row, <=256 streams}
+// (cp.async.bulk.tensor, 128B swizzle, no multicast) into a double-buffered shared-memory stage completed on
+// an mbarrier. The 128B swizzle puts chunk c of thread t's row at chunk c ^ (t & 7), so the 16-byte reads
+// of a quarter-warp hit eight different bank groups.
 //
-// Hash. h <- rol64(h,1) ^ S[in] ^ rol64(S[out], LEN) (hash_rot_sbox_pre_2.h:42-51 with the ring folded
-// into the outgoing byte, which is still in registers). S is kept in shared memory as 16 interleaved
-// copies, 8 bytes per entry, so the 16 lanes of each half-warp read disjoint banks whatever their bytes.
-// Bytes with the high bit set index entries that hold S[0] (ffbf.cpp:127-130).
+// Hash. h <- rol64(h,1) ^ S[in] ^ rol64(S[out], LEN) (hash_rot_sbox_pre_2.h:42-51 with the ring folded into
+// the outgoing byte, still in registers), on two 32-bit halves. S sits in shared memory as 16 interleaved
+// copies of 8-byte entries, so the 16 lanes of each half-warp read disjoint banks whatever their bytes. Bytes
+// with the high bit set index entries that hold S[0] (ffbf.cpp:127-130).
 //
-// Probes. The first S index functions (h1, h2 & (C-1)) are tested against a shared-memory copy of the
-// cache region (C <= 2^20 bits) or against an exact OR-summary of it (bit j = OR of cache bits
-// [j<<sh, (j+1)<<sh)), which can only reject windows the full test rejects. Windows that pass go to the
-// full K-bit test on the global bit array, in the reference order (checkInFilter, ffbf.cpp:214-239).
+// Probes. Stage 1 tests the first index function, h1 & (C-1), against a shared-memory table: the cache
+// region itself when it fits, else its OR-summary (bit j = OR of cache bits [j<<sh, (j+1)<<sh)), which only
+// rejects windows the full test rejects. A window that passes (and holds no '\n') is appended to its warp's
+// candidate queue in shared memory; full queues and row ends are flushed by the whole warp, each lane taking
+// queued candidates and running the full K-bit test on the global filter in the reference order
+// (checkInFilter, ffbf.cpp:214-239). The queue keeps the per-byte path free of branches that wait on L2.
 //
 // Validity. A window is tested only when its LEN bytes hold no '\n' (processFile resets the hash at '\n').
-// The position of the last '\n' is tracked per thread; its first and last '\n' per stream feed the
-// per-16 KiB-tile newline summaries the line resolver uses.
+// The last '\n' is tracked per thread; each stream's first and last '\n' feed the per-16 KiB-tile newline
+// summaries the line resolver reads.
 //
 // Every mbarrier wait is bounded; on timeout the CTA records an error flag and stops.
 #include <cuda.h>
@@ -36,17 +38,17 @@ namespace ffbf {
 
 namespace {
 
-constexpr int kFastThreads = 256;
 constexpr int kRowBytes = 128;
-constexpr int kStageBytes = kFastThreads * kRowBytes;  // 32 KiB per stage
-constexpr int kTabBytes = 256 * 16 * 8;                // 32 KiB: 16 copies of the S-box
-constexpr uint32_t kMaxCacheWords = (1u << 20) / 32;   // 128 KiB of cache copy / summary
+constexpr int kTabBytes = 256 * 16 * 8;  // 16 copies of the 256-entry S-box
+constexpr int kQueueCap = 64;            // candidates per warp queue
+constexpr int kQueueBytes = kQueueCap * 16;
 constexpr uint32_t kWaitLimit = 1u << 24;
+constexpr size_t kSmemLimit = 232448;    // opt-in shared memory per block on sm_100
 
 struct FastArgs {
     uint64_t n_streams;      // streams covered by the tensor map
     uint32_t rows;           // rows per stream
-    uint32_t n_supertiles;   // ceil(n_streams / kFastThreads)
+    uint32_t n_supertiles;   // ceil(n_streams / THREADS)
     uint32_t streams_per_tile_log2;  // log2(16384 / (rows * 128))
     Geom g;
     const uint32_t* main_words;
@@ -91,18 +93,48 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         : "memory");
 }
 
-__device__ __forceinline__ uint32_t byte_of(const uint32_t (&w)[32], int pos) {
-    return (w[pos >> 2] >> (8 * (pos & 3))) & 0xFFu;
+// Shared-memory loads the compiler may schedule freely (the tables are read-only after set-up, and every
+// later write to the stages is ordered by __syncthreads).
+__device__ __forceinline__ uint2 lds64(uint32_t addr) {
+    uint2 v;
+    asm("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
+    return v;
+}
+__device__ __forceinline__ uint32_t lds32(uint32_t addr) {
+    uint32_t v;
+    asm("ld.shared.u32 %0, [%1];" : "=r"(v) : "r"(addr));
+    return v;
 }
 
+// Global load of one filter word when `pred` holds (0 otherwise); read-only path.
+__device__ __forceinline__ uint32_t ldg_if(const uint32_t* p, bool pred) {
+    uint32_t v;
+    asm("{\n\t.reg .pred q;\n\tsetp.ne.u32 q, %2, 0;\n\tmov.u32 %0, 0;\n\t@q ld.global.nc.u32 %0, [%1];\n\t}"
+        : "=r"(v)
+        : "l"(p), "r"((uint32_t)pred));
+    return v;
+}
 
-template <int L>
-__device__ __forceinline__ uint64_t rolL(uint64_t x) {
-    return L == 32 ? ((x << 32) | (x >> 32)) : ((x << L) | (x >> (64 - L)));
+// byte i (0..3) of w, zero-extended
+__device__ __forceinline__ uint32_t byte_at(uint32_t w, int i) { return __byte_perm(w, 0u, 0x4440u + (uint32_t)i); }
+
+// rol64 of (hi:lo) by N, 0 < N < 64, on 32-bit halves
+template <int N>
+__device__ __forceinline__ void rol_pair(uint32_t lo, uint32_t hi, uint32_t& rlo, uint32_t& rhi) {
+    if (N == 32) {
+        rlo = hi;
+        rhi = lo;
+    } else if (N < 32) {
+        rlo = __funnelshift_l(hi, lo, N);
+        rhi = __funnelshift_l(lo, hi, N);
+    } else {
+        rlo = __funnelshift_l(lo, hi, N - 32);
+        rhi = __funnelshift_l(hi, lo, N - 32);
+    }
 }
 
 // Full K-bit test on the global main filter, reference order, early exit.
-__device__ __noinline__ bool full_check(const Geom g, const uint32_t* __restrict__ words, uint64_t h) {
+__device__ __forceinline__ bool full_check(const Geom& g, const uint32_t* __restrict__ words, uint64_t h) {
     for (uint32_t i = 0; i < g.k; i++) {
         uint32_t b = bit_index<1>(g, h, i);
         if (!((__ldg(words + (b >> 5)) >> (b & 31)) & 1u)) return false;
@@ -110,43 +142,61 @@ __device__ __noinline__ bool full_check(const Geom g, const uint32_t* __restrict
     return true;
 }
 
-__device__ __noinline__ void record_hit(const Geom g, uint32_t* ff_words, HitRec* hits, uint32_t cap,
-                                       uint32_t* counters, uint64_t start, uint64_t h) {
-    set_all<2>(g, ff_words, h);
-    uint32_t slot = atomicAdd(counters + CNT_HITS, 1u);
-    if (slot < cap) hits[slot] = HitRec{start, h};
-}
-
-// First '\n' position (0..127) in a row held as 32 words, or -1.
-__device__ __forceinline__ int first_newline(const uint32_t (&w)[32]) {
-    for (int k = 0; k < 32; k++) {
-        uint32_t t = w[k] ^ 0x0A0A0A0Au;
-        uint32_t z = ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
-        if (z) return 4 * k + (__ffs(z) - 1) / 8;
+// The whole warp drains its candidate queue: lane i takes entries i, i+32, ...
+__device__ __noinline__ void flush_queue(const FastArgs& a, uint32_t qaddr, int qn, uint64_t warp_row_pos0,
+                                         uint64_t row_stride, int lane) {
+    const Geom g = a.g;
+    for (int i = lane; i < qn; i += 32) {
+        uint4 e;
+        asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                     : "=r"(e.x), "=r"(e.y), "=r"(e.z), "=r"(e.w)
+                     : "r"(qaddr + 16u * (uint32_t)i));
+        const uint64_t h = ((uint64_t)e.z << 32) | e.y;
+        if (full_check(g, a.main_words, h)) {
+            const uint32_t owner = e.x >> 8, p = e.x & 0xFFu;
+            const uint64_t start = warp_row_pos0 + owner * row_stride + p + 1 - g.len;
+            set_all<2>(g, a.ff_words, h);
+            const uint32_t slot = atomicAdd(a.counters + CNT_HITS, 1u);
+            if (slot < a.hits_cap) a.hits[slot] = HitRec{start, h};
+        }
     }
-    return -1;
+    __syncwarp();
 }
 
-template <int L>
-__global__ void __launch_bounds__(kFastThreads, 1) k_scan_fast(const __grid_constant__ CUtensorMap tmap, FastArgs a) {
+// MODE 0 (sparse filters): stage 1 in shared memory, candidates queued per byte.
+// MODE 1 (dense filters, where a shared-memory summary would pass most windows): the exact h1 probe is a
+// global load issued for every valid window and consumed kRing bytes later from a register ring, so the
+// L2 latency overlaps the hashing of the next windows; windows whose h1 bit is set go to the queue.
+template <int L, int THREADS, int MODE>
+__global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant__ CUtensorMap tmap,
+                                                          const __grid_constant__ FastArgs a) {
+    constexpr int kStageBytes = THREADS * kRowBytes;
+    constexpr int kQCap = MODE == 0 ? kQueueCap : 2 * kQueueCap;
+    constexpr int kQBytes = kQCap * 16;
+    constexpr int kRing = 8;
+    constexpr int kBox = THREADS > 256 ? THREADS / 2 : THREADS;  // streams per TMA box (<= 256)
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t* smem = smem_raw + (base - raw);
-    const uint32_t stage0 = base;                       // 2 stages
-    uint64_t* tab = reinterpret_cast<uint64_t*>(smem + 2 * kStageBytes);
-    uint64_t* bars = reinterpret_cast<uint64_t*>(smem + 2 * kStageBytes + kTabBytes);
-    uint32_t* s1 = reinterpret_cast<uint32_t*>(smem + 2 * kStageBytes + kTabBytes + 128);
+    // layout: [stage 0][stage 1][S tables][mbarriers (128 B)][warp queues][stage-1 table]
+    const uint32_t stage0 = base;
+    const uint32_t tab = base + 2 * kStageBytes;
+    const uint32_t bar0 = tab + kTabBytes, bar1 = bar0 + 8;
+    const uint32_t queues = bar0 + 128;
+    const uint32_t s1 = queues + (THREADS / 32) * kQBytes;
     __shared__ int s_abort;
 
-    const int tid = threadIdx.x;
-    const int lane = tid & 31;
-    for (int i = tid; i < 256 * 16; i += kFastThreads) {
-        int c = i >> 4;
-        tab[i] = c_sbox[(c & 0x80) ? 0 : c];
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    {
+        uint64_t* tp = reinterpret_cast<uint64_t*>(smem + 2 * kStageBytes);
+        for (int i = tid; i < 256 * 16; i += THREADS) {
+            const int c = i >> 4;
+            tp[i] = c_sbox[(c & 0x80) ? 0 : c];
+        }
+        uint32_t* sp = reinterpret_cast<uint32_t*>(smem + (s1 - base));
+        for (uint32_t i = tid; i < a.stage1_nwords; i += THREADS) sp[i] = a.stage1_words[i];
     }
-    for (uint32_t i = tid; i < a.stage1_nwords; i += kFastThreads) s1[i] = a.stage1_words[i];
-    const uint32_t bar0 = smem_u32(bars), bar1 = bar0 + 8;
     if (tid == 0) {
         s_abort = 0;
         mbar_init(bar0, 1);
@@ -161,25 +211,56 @@ __global__ void __launch_bounds__(kFastThreads, 1) k_scan_fast(const __grid_cons
     uint32_t my_st = 0;
     if (blockIdx.x < a.n_supertiles) my_st = (a.n_supertiles - 1 - blockIdx.x) / gridDim.x + 1;
     const uint32_t total = my_st * per_st;
-    const uint64_t* lane_tab = tab + (lane & 15);  // entry c of this lane's copy: lane_tab[c * 16]
+    const uint32_t lane_tab = tab + (uint32_t)(lane & 15) * 8u;  // entry c of this lane's copy: + c * 128
     const uint32_t cmask = g.cache_mask;
     const uint32_t sh = a.stage1_shift;
-    const uint32_t* s1w = s1;
+    const uint32_t s1_amask = ((cmask >> sh) >> 3) & ~3u;  // byte offset mask of a stage-1 word
+    const uint32_t qaddr = queues + (uint32_t)warp * kQBytes;
+    const unsigned lt_mask = (1u << lane) - 1u;
 
     auto issue = [&](uint32_t k) {
         const uint32_t st = blockIdx.x + (k / per_st) * gridDim.x;
         const int r = (int)(k % per_st) - 1;
         const int y = r < 0 ? (int)R - 1 : r;
-        const int z = (int)(st * kFastThreads) + (r < 0 ? -1 : 0);
+        const int z = (int)(st * THREADS) + (r < 0 ? -1 : 0);
         const uint32_t bar = (k & 1) ? bar1 : bar0;
+        const uint32_t dst = stage0 + (k & 1) * kStageBytes;
         mbar_expect_tx(bar, kStageBytes);
-        tma_load_3d(stage0 + (k & 1) * kStageBytes, &tmap, 0, y, z, bar);
+        for (int b = 0; b < THREADS / kBox; b++) tma_load_3d(dst + b * kBox * kRowBytes, &tmap, 0, y, z + b * kBox, bar);
     };
 
     if (tid == 0 && total > 0) issue(0);
 
-    uint64_t h = 0;
-    int lnp = -1000;               // last '\n' relative to the current row start
+    int qn = 0;  // warp-uniform queue fill
+    uint64_t warp_row_pos0 = 0, row_stride = 0;
+    // Appends the lanes with `pass` to the warp queue; flushes when fewer than 32 slots remain.
+    auto enqueue = [&](bool pass, uint32_t pos, uint32_t ql, uint32_t qh) {
+        const unsigned m = __ballot_sync(0xffffffffu, pass);
+        if (m) {
+            if (pass) {
+                const uint32_t slot = (uint32_t)qn + __popc(m & lt_mask);
+                asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(qaddr + 16u * slot),
+                             "r"(pos | ((uint32_t)lane << 8)), "r"(ql), "r"(qh), "r"(0u)
+                             : "memory");
+            }
+            qn += __popc(m);
+            if (qn > kQCap - 32) {
+                __syncwarp();
+                flush_queue(a, qaddr, qn, warp_row_pos0, row_stride, lane);
+                qn = 0;
+            }
+        }
+    };
+    uint32_t ring_v[kRing], ring_l[kRing], ring_h[kRing];
+    int ring_p[kRing];
+#pragma unroll
+    for (int q = 0; q < kRing; q++) {
+        ring_v[q] = ring_l[q] = ring_h[q] = 0;
+        ring_p[q] = -1;
+    }
+
+    uint32_t hl = 0, hh = 0;
+    int lnp = -1000;  // last '\n' relative to the current row start
     long long first_nl = LLONG_MAX, last_nl = -1;
     uint32_t prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
@@ -207,7 +288,7 @@ __global__ void __launch_bounds__(kFastThreads, 1) k_scan_fast(const __grid_cons
 
         const uint32_t st = blockIdx.x + (k / per_st) * gridDim.x;
         const int r = (int)(k % per_st) - 1;
-        const uint64_t z = (uint64_t)st * kFastThreads + tid;
+        const uint64_t z = (uint64_t)st * THREADS + tid;
         const bool active = z < a.n_streams;
         const uint8_t* row = smem + (k & 1) * kStageBytes + tid * kRowBytes;
         const int sw = tid & 7;
@@ -218,57 +299,108 @@ __global__ void __launch_bounds__(kFastThreads, 1) k_scan_fast(const __grid_cons
             const uint4 c7 = *reinterpret_cast<const uint4*>(row + ((7 ^ sw) << 4));
             prev[0] = c6.x; prev[1] = c6.y; prev[2] = c6.z; prev[3] = c6.w;
             prev[4] = c7.x; prev[5] = c7.y; prev[6] = c7.z; prev[7] = c7.w;
-            h = 0;
+            hl = 0;
+            hh = 0;
             lnp = -1000;
 #pragma unroll
             for (int j = 0; j < 32; j++) {
-                const uint32_t c = (prev[j >> 2] >> (8 * (j & 3))) & 0xFFu;
-                h = rol64(h, 1) ^ lane_tab[c * 16];
+                const uint32_t c = byte_at(prev[j >> 2], j & 3);
+                const uint2 s = lds64(lane_tab + c * 128u);
+                uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
+                nl ^= s.x;
+                nh ^= s.y;
                 if (j >= L) {
-                    const uint32_t co = (prev[(j - L) >> 2] >> (8 * ((j - L) & 3))) & 0xFFu;
-                    h ^= rolL<L>(lane_tab[co * 16]);
+                    const uint32_t co = byte_at(prev[(j - L) >> 2], (j - L) & 3);
+                    const uint2 o = lds64(lane_tab + co * 128u);
+                    uint32_t rl, rh;
+                    rol_pair<L>(o.x, o.y, rl, rh);
+                    nl ^= rl;
+                    nh ^= rh;
                 }
+                hl = nl;
+                hh = nh;
                 if (c == 0x0Au) lnp = j - 32;
             }
             if (z == 0) lnp = -1;  // text start: nothing before offset 0
             first_nl = LLONG_MAX;
             last_nl = -1;
         } else {
-            uint32_t w[32];
+            const int lnp_in = lnp;
+            qn = 0;
+            warp_row_pos0 = ((uint64_t)st * THREADS + (uint64_t)warp * 32) * R * kRowBytes + (uint64_t)r * kRowBytes;
+            row_stride = (uint64_t)R * kRowBytes;
+            int row_first = -1;  // first '\n' of this row, found once per stream
+#pragma unroll 1
+            for (int b = 0; b < kRowBytes / 32; b++) {
+                uint32_t cur[8];
+                {
+                    const uint4 v0 = *reinterpret_cast<const uint4*>(row + (((2 * b) ^ sw) << 4));
+                    const uint4 v1 = *reinterpret_cast<const uint4*>(row + (((2 * b + 1) ^ sw) << 4));
+                    cur[0] = v0.x; cur[1] = v0.y; cur[2] = v0.z; cur[3] = v0.w;
+                    cur[4] = v1.x; cur[5] = v1.y; cur[6] = v1.z; cur[7] = v1.w;
+                }
+                const int lnp_blk = lnp;
 #pragma unroll
-            for (int c = 0; c < 8; c++) {
-                const uint4 v = *reinterpret_cast<const uint4*>(row + ((c ^ sw) << 4));
-                w[4 * c] = v.x; w[4 * c + 1] = v.y; w[4 * c + 2] = v.z; w[4 * c + 3] = v.w;
-            }
-            if (active) {
-                const long long row_pos = (long long)(z * R + (uint32_t)r) * kRowBytes;
-                const int lnp_in = lnp;
-#pragma unroll
-                for (int p = 0; p < kRowBytes; p++) {
-                    const uint32_t c = byte_of(w, p);
+                for (int j = 0; j < 32; j++) {
+                    const uint32_t c = byte_at(cur[j >> 2], j & 3);
                     uint32_t co;
-                    if (p >= L) co = byte_of(w, p - L);
-                    else co = (prev[(p - L + 32) >> 2] >> (8 * ((p - L + 32) & 3))) & 0xFFu;
-                    h = rol64(h, 1) ^ lane_tab[c * 16] ^ rolL<L>(lane_tab[co * 16]);
-                    if (c == 0x0Au) lnp = p;
-                    if (p - lnp >= L) {
-                        const uint32_t i0 = ((uint32_t)h & cmask) >> sh;
-                        bool pass = (s1w[i0 >> 5] >> (i0 & 31)) & 1u;
-                        if (pass && g.s > 1) {
-                            const uint32_t i1 = ((uint32_t)(h >> 32) & cmask) >> sh;
-                            pass = (s1w[i1 >> 5] >> (i1 & 31)) & 1u;
-                        }
-                        if (pass && full_check(g, a.main_words, h))
-                            record_hit(g, a.ff_words, a.hits, a.hits_cap, a.counters, (uint64_t)(row_pos + p + 1 - L), h);
+                    if (j >= L) co = byte_at(cur[(j - L) >> 2], (j - L) & 3);
+                    else co = byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
+                    const uint2 s = lds64(lane_tab + c * 128u);
+                    const uint2 o = lds64(lane_tab + co * 128u);
+                    uint32_t rl, rh;
+                    rol_pair<L>(o.x, o.y, rl, rh);
+                    const uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
+                    hl = nl ^ s.x ^ rl;
+                    hh = nh ^ s.y ^ rh;
+                    if (c == 0x0Au) lnp = j;
+                    if constexpr (MODE == 0) {
+                        const uint32_t hs = hl >> sh;
+                        const uint32_t word = lds32(s1 + ((hs >> 3) & s1_amask));
+                        const bool pass = active && (j - lnp >= L) && ((__funnelshift_r(word, word, hs) & 1u) != 0);
+                        enqueue(pass, (uint32_t)(32 * b + j), hl, hh);
+                    } else {
+                        const int slot = j % kRing;
+                        // the window issued kRing bytes ago: its h1 word has arrived by now
+                        const bool pass = ring_p[slot] >= 0 &&
+                                          ((__funnelshift_r(ring_v[slot], ring_v[slot], ring_l[slot]) & 1u) != 0);
+                        enqueue(pass, (uint32_t)ring_p[slot], ring_l[slot], ring_h[slot]);
+                        const bool valid = active && (j - lnp >= L);
+                        ring_l[slot] = hl;
+                        ring_h[slot] = hh;
+                        ring_p[slot] = valid ? 32 * b + j : -1;
+                        ring_v[slot] = ldg_if(a.main_words + ((hl & cmask) >> 5), valid);
                     }
                 }
-                if (lnp != lnp_in) {
-                    if (first_nl == LLONG_MAX) first_nl = row_pos + first_newline(w);
-                    last_nl = row_pos + lnp;
+                if (lnp != lnp_blk && row_first < 0 && first_nl == LLONG_MAX) {
+                    for (int k = 0; k < 8 && row_first < 0; k++) {
+                        const uint32_t t = cur[k] ^ 0x0A0A0A0Au;
+                        const uint32_t zb = ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
+                        if (zb) row_first = 32 * b + 4 * k + (__ffs(zb) - 1) / 8;
+                    }
                 }
-                lnp -= kRowBytes;
+                lnp -= 32;
 #pragma unroll
-                for (int q = 0; q < 8; q++) prev[q] = w[24 + q];
+                for (int q = 0; q < 8; q++) prev[q] = cur[q];
+            }
+            if constexpr (MODE == 1) {
+#pragma unroll
+                for (int q = 0; q < kRing; q++) {  // drain the ring before the row's buffer is released
+                    const bool pass = ring_p[q] >= 0 && ((__funnelshift_r(ring_v[q], ring_v[q], ring_l[q]) & 1u) != 0);
+                    enqueue(pass, (uint32_t)ring_p[q], ring_l[q], ring_h[q]);
+                    ring_p[q] = -1;
+                }
+            }
+            if (qn) {
+                __syncwarp();
+                flush_queue(a, qaddr, qn, warp_row_pos0, row_stride, lane);
+                qn = 0;
+            }
+            // lnp is now relative to the next row's start; lnp + 128 is its position in this row
+            if (active && lnp + kRowBytes != lnp_in) {
+                const long long row_pos = (long long)(z * R + (uint32_t)r) * kRowBytes;
+                if (first_nl == LLONG_MAX) first_nl = row_pos + row_first;
+                last_nl = row_pos + lnp + kRowBytes;
             }
             if ((uint32_t)r == R - 1) {
                 // per-16 KiB-tile newline summary: reduce over the lanes whose streams share the tile
@@ -301,16 +433,58 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     return fn;
 }
 
-template <int L>
-cudaError_t launch_len(const CUtensorMap& map, const FastArgs& fa, int grid, size_t smem, cudaStream_t st) {
-    cudaError_t e = cudaFuncSetAttribute(k_scan_fast<L>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+template <int THREADS, int MODE>
+constexpr size_t fixed_smem() {
+    return 1024 + 2 * (size_t)THREADS * kRowBytes + kTabBytes + 128 +
+           (THREADS / 32) * (size_t)(MODE == 0 ? kQueueBytes : 2 * kQueueBytes);
+}
+
+template <int L, int THREADS, int MODE>
+cudaError_t launch_cfg(const CUtensorMap& map, const FastArgs& fa, int num_sms, cudaStream_t st) {
+    const size_t smem = fixed_smem<THREADS, MODE>() + 4 * (size_t)fa.stage1_nwords;
+    cudaError_t e =
+        cudaFuncSetAttribute(k_scan_fast<L, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    k_scan_fast<L><<<grid, kFastThreads, smem, st>>>(map, fa);
+    const int grid = (int)(fa.n_supertiles < (uint32_t)num_sms ? fa.n_supertiles : (uint32_t)num_sms);
+    k_scan_fast<L, THREADS, MODE><<<grid, THREADS, smem, st>>>(map, fa);
     note_launches(1);
     return cudaGetLastError();
 }
 
+template <int L>
+cudaError_t launch_len(int threads, int mode, const CUtensorMap& map, const FastArgs& fa, int num_sms,
+                       cudaStream_t st) {
+    if (mode == 1) return launch_cfg<L, 512, 1>(map, fa, num_sms, st);
+    switch (threads) {
+        case 256: return launch_cfg<L, 256, 0>(map, fa, num_sms, st);
+        case 384: return launch_cfg<L, 384, 0>(map, fa, num_sms, st);
+        default: return launch_cfg<L, 512, 0>(map, fa, num_sms, st);
+    }
+}
+
+size_t fixed_smem_for(int threads) {
+    switch (threads) {
+        case 256: return fixed_smem<256, 0>();
+        case 384: return fixed_smem<384, 0>();
+        default: return fixed_smem<512, 0>();
+    }
+}
+
+int g_threads_override = 0;
+
+// Largest power-of-two stage-1 table (in bits, <= C) that fits beside the fixed shared-memory layout.
+uint32_t stage1_shift_for_threads(const Geom& g, int threads) {
+    const size_t room = kSmemLimit - fixed_smem_for(threads) - 64;
+    uint32_t sh = 0;
+    while (((uint64_t)g.cache_bits >> sh) / 8 > room) sh++;
+    return sh;
+}
+
 }  // namespace
+
+int fast_scan_threads() { return g_threads_override ? g_threads_override : 384; }
+
+void set_fast_scan_threads(int t) { g_threads_override = (t == 256 || t == 384 || t == 512) ? t : 0; }
 
 bool fast_scan_supported(const Geom& g, uint64_t n) {
     switch (g.len) {
@@ -322,23 +496,20 @@ bool fast_scan_supported(const Geom& g, uint64_t n) {
     return encoder() != nullptr;
 }
 
-uint32_t stage1_shift_for(const Geom& g) {
-    uint32_t sh = 0;
-    while (((uint64_t)g.cache_bits >> sh) > (uint64_t)kMaxCacheWords * 32) sh++;
-    return sh;
-}
+uint32_t stage1_shift_for(const Geom& g) { return stage1_shift_for_threads(g, fast_scan_threads()); }
 
-cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int num_sms, cudaStream_t st) {
+cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int mode, int num_sms, cudaStream_t st) {
+    const int threads = mode == 1 ? 512 : fast_scan_threads();
     const uint64_t fast_tiles = a.n / kScanTile;  // whole 16 KiB tiles; the rest goes to the generic kernel
     // rows per stream: the largest power of two (<= 16) that still gives every SM several supertiles
     uint32_t rows = 16;
-    while (rows > 4 && fast_tiles * kScanTile / ((uint64_t)rows * kRowBytes * kFastThreads) < 4ull * num_sms) rows >>= 1;
+    while (rows > 4 && fast_tiles * kScanTile / ((uint64_t)rows * kRowBytes * threads) < 4ull * num_sms) rows >>= 1;
     const uint64_t slen = (uint64_t)rows * kRowBytes;
     const uint64_t n_streams = fast_tiles * kScanTile / slen;
     FastArgs fa{};
     fa.n_streams = n_streams;
     fa.rows = rows;
-    fa.n_supertiles = (uint32_t)((n_streams + kFastThreads - 1) / kFastThreads);
+    fa.n_supertiles = (uint32_t)((n_streams + threads - 1) / threads);
     uint32_t spt = (uint32_t)(kScanTile / slen), lg = 0;
     while ((1u << lg) < spt) lg++;
     fa.streams_per_tile_log2 = lg;
@@ -346,8 +517,8 @@ cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int num_s
     fa.main_words = a.main_words;
     fa.ff_words = a.ff_words;
     fa.stage1_words = stage1_words;
-    fa.stage1_shift = stage1_shift_for(a.g);
-    fa.stage1_nwords = (uint32_t)(((uint64_t)a.g.cache_bits >> fa.stage1_shift) / 32);
+    fa.stage1_shift = mode == 1 ? 0 : stage1_shift_for_threads(a.g, threads);
+    fa.stage1_nwords = mode == 1 ? 0 : (uint32_t)(((uint64_t)a.g.cache_bits >> fa.stage1_shift) / 32);
     fa.hits = a.hits;
     fa.hits_cap = a.hits_cap;
     fa.counters = a.counters;
@@ -356,28 +527,27 @@ cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int num_s
 
     if (n_streams > 0) {
         CUtensorMap map;
+        const uint32_t box_streams = threads > 256 ? (uint32_t)threads / 2 : (uint32_t)threads;
         cuuint64_t dims[3] = {(cuuint64_t)kRowBytes, (cuuint64_t)rows, (cuuint64_t)n_streams};
         cuuint64_t strides[2] = {(cuuint64_t)kRowBytes, (cuuint64_t)slen};
-        cuuint32_t box[3] = {(cuuint32_t)kRowBytes, 1u, (cuuint32_t)kFastThreads};
+        cuuint32_t box[3] = {(cuuint32_t)kRowBytes, 1u, box_streams};
         cuuint32_t estr[3] = {1u, 1u, 1u};
         CUresult cr = encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)a.text, dims, strides, box, estr,
                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
         if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
-        const size_t smem = 1024 + 2 * kStageBytes + kTabBytes + 128 + 4 * (size_t)fa.stage1_nwords;
-        const int grid = (int)(fa.n_supertiles < (uint32_t)num_sms ? fa.n_supertiles : (uint32_t)num_sms);
         cudaError_t e;
         switch (a.g.len) {
-            case 16: e = launch_len<16>(map, fa, grid, smem, st); break;
-            case 19: e = launch_len<19>(map, fa, grid, smem, st); break;
-            case 20: e = launch_len<20>(map, fa, grid, smem, st); break;
-            case 24: e = launch_len<24>(map, fa, grid, smem, st); break;
-            case 32: e = launch_len<32>(map, fa, grid, smem, st); break;
+            case 16: e = launch_len<16>(threads, mode, map, fa, num_sms, st); break;
+            case 19: e = launch_len<19>(threads, mode, map, fa, num_sms, st); break;
+            case 20: e = launch_len<20>(threads, mode, map, fa, num_sms, st); break;
+            case 24: e = launch_len<24>(threads, mode, map, fa, num_sms, st); break;
+            case 32: e = launch_len<32>(threads, mode, map, fa, num_sms, st); break;
             default: return cudaErrorInvalidValue;
         }
         if (e != cudaSuccess) return e;
     }
-    // the partial last tile (and anything the streams did not cover) through the generic kernel
+    // the partial last tile through the generic kernel
     const uint64_t ntiles = (a.n + kScanTile - 1) / kScanTile;
     if (fast_tiles < ntiles) {
         ScanArgs t = a;
@@ -391,8 +561,7 @@ cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int num_s
 }
 
 // Summary of the cache region for the stage-1 test: bit j = OR of cache bits [j << sh, (j + 1) << sh).
-__global__ void k_stage1_summary(const uint32_t* main_words, uint32_t cache_bits, uint32_t sh, uint32_t* out,
-                                 uint32_t nwords) {
+__global__ void k_stage1_summary(const uint32_t* main_words, uint32_t sh, uint32_t* out, uint32_t nwords) {
     uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= nwords) return;
     uint32_t v = 0;
@@ -411,18 +580,36 @@ __global__ void k_stage1_summary(const uint32_t* main_words, uint32_t cache_bits
         v |= (uint32_t)any << b;
     }
     out[w] = v;
-    (void)cache_bits;
 }
 
 cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, uint32_t* out, cudaStream_t st) {
     const uint32_t sh = stage1_shift_for(g);
     const uint32_t nwords = (uint32_t)(((uint64_t)g.cache_bits >> sh) / 32);
     if (sh == 0) return cudaMemcpyAsync(out, main_words, 4ull * nwords, cudaMemcpyDeviceToDevice, st);
-    k_stage1_summary<<<(nwords + 255) / 256, 256, 0, st>>>(main_words, g.cache_bits, sh, out, nwords);
+    k_stage1_summary<<<(nwords + 255) / 256, 256, 0, st>>>(main_words, sh, out, nwords);
     note_launches(1);
     return cudaGetLastError();
 }
 
 uint32_t stage1_words_for(const Geom& g) { return (uint32_t)(((uint64_t)g.cache_bits >> stage1_shift_for(g)) / 32); }
+
+}  // namespace ffbf
+
+namespace ffbf {
+
+__global__ void k_popcount(const uint32_t* w, uint32_t n, unsigned long long* out) {
+    unsigned long long c = 0;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) c += __popc(w[i]);
+    for (int o = 16; o; o >>= 1) c += __shfl_xor_sync(0xffffffffu, c, o);
+    if ((threadIdx.x & 31) == 0 && c) atomicAdd(out, c);
+}
+
+cudaError_t popcount_words(const uint32_t* w, uint32_t n, unsigned long long* d_out, cudaStream_t st) {
+    cudaError_t e = cudaMemsetAsync(d_out, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess || n == 0) return e;
+    k_popcount<<<(n + 255) / 256 < 1024 ? (n + 255) / 256 : 1024, 256, 0, st>>>(w, n, d_out);
+    note_launches(1);
+    return cudaGetLastError();
+}
 
 }  // namespace ffbf

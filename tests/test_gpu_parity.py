@@ -173,16 +173,33 @@ def test_cli_matches_reference_files():
         assert r.stdout == g.stdout and len(g.stdout) > 0
 
 
-@pytest.mark.parametrize("name", ["plain_small", "scale_small", "smem_cache", "edge_chunks", "binary_small"])
-def test_generic_and_tuned_scans_agree(name, monkeypatch):
-    """The generic kernel (any geometry) and the tuned sm_100a kernel give identical results."""
+SCAN_VARIANTS = [
+    {"FFBF_FORCE_GENERIC_SCAN": "1"},
+    {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "256"},
+    {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "384"},
+    {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "512"},
+    {"FFBF_SCAN_MODE": "1"},
+]
+
+
+@pytest.mark.parametrize("name", ["plain_small", "scale_small", "smem_cache", "edge_chunks", "binary_small",
+                                  "dense_fp", "len19_default"])
+def test_scan_variants_agree_with_oracle(name, monkeypatch):
+    """Every scan kernel variant (generic; tuned sparse at each CTA size; tuned dense) is bit-exact."""
     prm, pats, text = build_inputs(name)
-    outs = []
-    for force in ("1", "0"):
-        monkeypatch.setenv("FFBF_FORCE_GENERIC_SCAN", force)
+    o, s, _, _, _ = run_oracle(prm, pats, text)
+    for env in SCAN_VARIANTS:
+        for k in ("FFBF_FORCE_GENERIC_SCAN", "FFBF_SCAN_MODE", "FFBF_SCAN_THREADS"):
+            monkeypatch.delenv(k, raising=False)
+        for k, v in env.items():
+            monkeypatch.setenv(k, v)
         with Filter(prm) as f:
             f.add_patterns(pats)
             r = f.process(text)
-            outs.append((r.hit_offsets, r.line_start, r.line_end, f.get_filters()[1]))
-    for a, b in zip(*outs):
-        np.testing.assert_array_equal(a, b)
+            np.testing.assert_array_equal(r.hit_offsets, s["hits"], err_msg=str(env))
+            np.testing.assert_array_equal(r.line_start, s["line_start"], err_msg=str(env))
+            np.testing.assert_array_equal(r.line_end, s["line_end"], err_msg=str(env))
+            np.testing.assert_array_equal(f.get_filters()[1], o.ff, err_msg=str(env))
+    monkeypatch.setenv("FFBF_SCAN_THREADS", "0")
+    with Filter(prm):
+        pass  # restores the default CTA size for later tests
