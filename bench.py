@@ -127,6 +127,17 @@ def gpu_id_for(dev):
         return vis.split(",")[dev] if vis else dev
 
 
+def profiled_traffic_ratio(workload_name):
+    """DRAM bytes per text byte of the scan kernel, from the committed ncu summary for this workload."""
+    path = os.path.join(ROOT, "profiles", f"k_scan_fast_dense_{workload_name}_256MiB.md")
+    if not os.path.exists(path):
+        return None
+    for line in open(path):
+        if line.startswith("| traffic_bytes_per_text_byte |"):
+            return float(line.split("|")[2])
+    return None
+
+
 def measured_peaks():
     p = os.path.join(ROOT, "MEASURED_PEAKS.json")
     if os.path.exists(p):
@@ -349,7 +360,9 @@ def main_ours(args):
         "vs_baseline": None, "dtype": "u8", "data": "synthetic",
         "config": dict(describe(wl), parallelism=f"replicas x{world}" if world > 1 else "single GPU"),
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                     "peak_source": f"{peak_kind} hbm_gbs",
+                     "traffic": (lambda r: None if r is None else r * n)(profiled_traffic_ratio(wl.name)),
+                     "traffic_source": "ncu dram bytes of a 256 MiB capture scaled to this text (profiles/)",
                      "algorithmic_bytes_per_launch": n},
         "e2e": {"value": world * n * e2e_steps / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": n,
                 "d2h_bytes_per_step": d2h // max(e2e_steps, 1),
