@@ -55,7 +55,7 @@ struct FastArgs {
     uint32_t* ff_words;
     const uint32_t* stage1_words;  // cache region copy or its summary (global), copied into smem
     uint32_t stage1_nwords;
-    uint32_t stage1_shift;         // index >> shift before the smem lookup (0: exact copy)
+    uint32_t stage1_shift;         // the table holds C >> shift bits (0: exact copy of the cache region)
     HitRec* hits;
     uint32_t hits_cap;
     uint32_t* counters;
@@ -121,10 +121,10 @@ __device__ __forceinline__ uint32_t byte_at(uint32_t w, int i) { return __byte_p
 // rol64 of (hi:lo) by N, 0 < N < 64, on 32-bit halves
 template <int N>
 __device__ __forceinline__ void rol_pair(uint32_t lo, uint32_t hi, uint32_t& rlo, uint32_t& rhi) {
-    if (N == 32) {
+    if constexpr (N == 32) {
         rlo = hi;
         rhi = lo;
-    } else if (N < 32) {
+    } else if constexpr (N < 32) {
         rlo = __funnelshift_l(hi, lo, N);
         rhi = __funnelshift_l(lo, hi, N);
     } else {
@@ -133,32 +133,55 @@ __device__ __forceinline__ void rol_pair(uint32_t lo, uint32_t hi, uint32_t& rlo
     }
 }
 
-// Full K-bit test on the global main filter, reference order, early exit.
-__device__ __forceinline__ bool full_check(const Geom& g, const uint32_t* __restrict__ words, uint64_t h) {
-    for (uint32_t i = 0; i < g.k; i++) {
+// Full test from probe FROM on (reference order, early exit); probes before FROM are known to be set.
+__device__ __forceinline__ bool full_check_from(const Geom& g, const uint32_t* __restrict__ words, uint64_t h,
+                                                uint32_t from) {
+    for (uint32_t i = from; i < g.k; i++) {
         uint32_t b = bit_index<1>(g, h, i);
         if (!((__ldg(words + (b >> 5)) >> (b & 31)) & 1u)) return false;
     }
     return true;
 }
 
-// The whole warp drains its candidate queue: lane i takes entries i, i+32, ...
-__device__ __noinline__ void flush_queue(const FastArgs& a, uint32_t qaddr, int qn, uint64_t warp_row_pos0,
-                                         uint64_t row_stride, int lane) {
-    const Geom g = a.g;
-    for (int i = lane; i < qn; i += 32) {
-        uint4 e;
-        asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
-                     : "=r"(e.x), "=r"(e.y), "=r"(e.z), "=r"(e.w)
-                     : "r"(qaddr + 16u * (uint32_t)i));
-        const uint64_t h = ((uint64_t)e.z << 32) | e.y;
-        if (full_check(g, a.main_words, h)) {
-            const uint32_t owner = e.x >> 8, p = e.x & 0xFFu;
-            const uint64_t start = warp_row_pos0 + owner * row_stride + p + 1 - g.len;
-            set_all<2>(g, a.ff_words, h);
-            const uint32_t slot = atomicAdd(a.counters + CNT_HITS, 1u);
-            if (slot < a.hits_cap) a.hits[slot] = HitRec{start, h};
+// The whole warp drains its candidate queue: lane i takes entries i, i+32, ... (PER_LANE at most). An entry
+// is {position | lane << 8, h1, h2, first}: probes before `first` are known to be set. Every lane issues the
+// probe `first` of all its entries before testing any, so its L2 round trips overlap; survivors finish the
+// test one by one.
+template <int PER_LANE>
+__device__ __noinline__ void flush_queue(const Geom g, const uint32_t* __restrict__ main_words, uint32_t* ff_words,
+                                         HitRec* hits, uint32_t hits_cap, uint32_t* counters, uint32_t qaddr, int qn,
+                                         uint64_t warp_row_pos0, uint64_t row_stride, int lane) {
+    uint4 e[PER_LANE];
+    uint32_t v[PER_LANE], bi[PER_LANE];
+#pragma unroll
+    for (int t = 0; t < PER_LANE; t++) {
+        const int i = lane + 32 * t;
+        e[t] = make_uint4(0, 0, 0, 0);
+        v[t] = 0xffffffffu;
+        bi[t] = 0;
+        if (i < qn) {
+            asm volatile("ld.shared.v4.u32 {%0, %1, %2, %3}, [%4];"
+                         : "=r"(e[t].x), "=r"(e[t].y), "=r"(e[t].z), "=r"(e[t].w)
+                         : "r"(qaddr + 16u * (uint32_t)i));
+            if (e[t].w < g.k) {
+                const uint64_t h = ((uint64_t)e[t].z << 32) | e[t].y;
+                bi[t] = bit_index<1>(g, h, e[t].w);
+                v[t] = __ldg(main_words + (bi[t] >> 5));
+            }
         }
+    }
+#pragma unroll
+    for (int t = 0; t < PER_LANE; t++) {
+        const int i = lane + 32 * t;
+        if (i >= qn) continue;
+        const uint64_t h = ((uint64_t)e[t].z << 32) | e[t].y;
+        if (!((v[t] >> (bi[t] & 31)) & 1u)) continue;
+        if (!full_check_from(g, main_words, h, e[t].w + 1)) continue;
+        const uint32_t owner = e[t].x >> 8, p = e[t].x & 0xFFu;
+        const uint64_t start = warp_row_pos0 + owner * row_stride + p + 1 - g.len;
+        set_all<2>(g, ff_words, h);
+        const uint32_t slot = atomicAdd(counters + CNT_HITS, 1u);
+        if (slot < hits_cap) hits[slot] = HitRec{start, h};
     }
     __syncwarp();
 }
@@ -173,7 +196,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
     constexpr int kStageBytes = THREADS * kRowBytes;
     constexpr int kQCap = MODE == 0 ? kQueueCap : 2 * kQueueCap;
     constexpr int kQBytes = kQCap * 16;
-    constexpr int kRing = 8;
+    constexpr int kRing = 8;             // dense mode: ring depth per stage (divides 32)
     constexpr int kBox = THREADS > 256 ? THREADS / 2 : THREADS;  // streams per TMA box (<= 256)
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -213,8 +236,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
     const uint32_t total = my_st * per_st;
     const uint32_t lane_tab = tab + (uint32_t)(lane & 15) * 8u;  // entry c of this lane's copy: + c * 128
     const uint32_t cmask = g.cache_mask;
-    const uint32_t sh = a.stage1_shift;
-    const uint32_t s1_amask = ((cmask >> sh) >> 3) & ~3u;  // byte offset mask of a stage-1 word
+    // stage-1 table of T = C >> shift bits, folded modulo T: the byte offset of bit (h & (T-1))'s word is
+    // (h >> 3) & s1_bmask
+    const uint32_t s1_bmask = (((cmask >> a.stage1_shift) >> 3) & ~3u);
+    const bool two = g.s > 1;
     const uint32_t qaddr = queues + (uint32_t)warp * kQBytes;
     const unsigned lt_mask = (1u << lane) - 1u;
 
@@ -234,30 +259,34 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
     int qn = 0;  // warp-uniform queue fill
     uint64_t warp_row_pos0 = 0, row_stride = 0;
     // Appends the lanes with `pass` to the warp queue; flushes when fewer than 32 slots remain.
-    auto enqueue = [&](bool pass, uint32_t pos, uint32_t ql, uint32_t qh) {
+    auto enqueue = [&](bool pass, uint32_t pos, uint32_t ql, uint32_t qh, uint32_t first) {
         const unsigned m = __ballot_sync(0xffffffffu, pass);
         if (m) {
             if (pass) {
                 const uint32_t slot = (uint32_t)qn + __popc(m & lt_mask);
                 asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(qaddr + 16u * slot),
-                             "r"(pos | ((uint32_t)lane << 8)), "r"(ql), "r"(qh), "r"(0u)
+                             "r"(pos | ((uint32_t)lane << 8)), "r"(ql), "r"(qh), "r"(first)
                              : "memory");
             }
             qn += __popc(m);
             if (qn > kQCap - 32) {
                 __syncwarp();
-                flush_queue(a, qaddr, qn, warp_row_pos0, row_stride, lane);
+                flush_queue<kQCap / 32>(g, a.main_words, a.ff_words, a.hits, a.hits_cap, a.counters, qaddr, qn,
+                                              warp_row_pos0, row_stride, lane);
                 qn = 0;
             }
         }
     };
-    uint32_t ring_v[kRing], ring_l[kRing], ring_h[kRing];
-    int ring_p[kRing];
+    // dense-mode rings. Stage A: the h1-probe word (0 when the window was not valid, so its test fails),
+    // h1, h2. Stage B: the second probe's word (0 when stage A failed), h1, h2.
+    constexpr int kR = MODE == 1 ? kRing : 1;
+    uint32_t ring_v[kR], ring_l[kR], ring_h[kR], ring2_v[kR], ring2_l[kR], ring2_h[kR];
 #pragma unroll
-    for (int q = 0; q < kRing; q++) {
-        ring_v[q] = ring_l[q] = ring_h[q] = 0;
-        ring_p[q] = -1;
-    }
+    for (int q = 0; q < kR; q++) ring_v[q] = ring_l[q] = ring_h[q] = ring2_v[q] = ring2_l[q] = ring2_h[q] = 0;
+    // second probe's index function (getHashValue case 1): cache region when S > 1, else external region
+    const uint32_t p2_mask = two ? cmask : g.ext_mask, p2_add = two ? 0u : g.cache_bits;
+    // sparse mode: the stage-1 probes are exact when the table is the cache region itself
+    const uint32_t s1_first = a.stage1_shift == 0 ? (two ? 2u : 1u) : 0u;
 
     uint32_t hl = 0, hh = 0;
     int lnp = -1000;  // last '\n' relative to the current row start
@@ -355,20 +384,26 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
                     hh = nh ^ s.y ^ rh;
                     if (c == 0x0Au) lnp = j;
                     if constexpr (MODE == 0) {
-                        const uint32_t hs = hl >> sh;
-                        const uint32_t word = lds32(s1 + ((hs >> 3) & s1_amask));
-                        const bool pass = active && (j - lnp >= L) && ((__funnelshift_r(word, word, hs) & 1u) != 0);
-                        enqueue(pass, (uint32_t)(32 * b + j), hl, hh);
+                        const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
+                        const uint32_t w1 = lds32(s1 + ((hh >> 3) & s1_bmask));
+                        const bool b0 = (__funnelshift_r(w0, w0, hl) & 1u) != 0;
+                        const bool b1 = (__funnelshift_r(w1, w1, hh) & 1u) != 0;
+                        const bool pass = active && (j - lnp >= L) && b0 && (b1 || !two);
+                        enqueue(pass, (uint32_t)(32 * b + j), hl, hh, s1_first);
                     } else {
                         const int slot = j % kRing;
-                        // the window issued kRing bytes ago: its h1 word has arrived by now
-                        const bool pass = ring_p[slot] >= 0 &&
-                                          ((__funnelshift_r(ring_v[slot], ring_v[slot], ring_l[slot]) & 1u) != 0);
-                        enqueue(pass, (uint32_t)ring_p[slot], ring_l[slot], ring_h[slot]);
+                        // stage B: the window that entered stage A 2*kRing bytes ago
+                        // (the second probe's bit sits at h2 & 31 in its word for both index functions)
+                        const bool pass2 = (__funnelshift_r(ring2_v[slot], ring2_v[slot], ring2_h[slot]) & 1u) != 0;
+                        enqueue(pass2, (uint32_t)(32 * b + j - 2 * kRing), ring2_l[slot], ring2_h[slot], 2u);
+                        // stage A: the window issued kRing bytes ago; its h1 word has arrived by now
+                        const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], ring_l[slot]) & 1u) != 0;
+                        ring2_l[slot] = ring_l[slot];
+                        ring2_h[slot] = ring_h[slot];
+                        ring2_v[slot] = ldg_if(a.main_words + (((ring_h[slot] & p2_mask) + p2_add) >> 5), pass1);
                         const bool valid = active && (j - lnp >= L);
                         ring_l[slot] = hl;
                         ring_h[slot] = hh;
-                        ring_p[slot] = valid ? 32 * b + j : -1;
                         ring_v[slot] = ldg_if(a.main_words + ((hl & cmask) >> 5), valid);
                     }
                 }
@@ -385,15 +420,21 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
             }
             if constexpr (MODE == 1) {
 #pragma unroll
-                for (int q = 0; q < kRing; q++) {  // drain the ring before the row's buffer is released
-                    const bool pass = ring_p[q] >= 0 && ((__funnelshift_r(ring_v[q], ring_v[q], ring_l[q]) & 1u) != 0);
-                    enqueue(pass, (uint32_t)ring_p[q], ring_l[q], ring_h[q]);
-                    ring_p[q] = -1;
+                // drain: stage-B slot q holds the window ending at 128 - 2*kRing + q, stage-A slot q the one at
+                // 128 - kRing + q; stage-A survivors go to the queue with only their first probe known
+                for (int q = 0; q < kRing; q++) {
+                    const bool pass2 = (__funnelshift_r(ring2_v[q], ring2_v[q], ring2_h[q]) & 1u) != 0;
+                    enqueue(pass2, (uint32_t)(kRowBytes - 2 * kRing + q), ring2_l[q], ring2_h[q], 2u);
+                    const bool pass1 = (__funnelshift_r(ring_v[q], ring_v[q], ring_l[q]) & 1u) != 0;
+                    enqueue(pass1, (uint32_t)(kRowBytes - kRing + q), ring_l[q], ring_h[q], 1u);
+                    ring_v[q] = 0;
+                    ring2_v[q] = 0;
                 }
             }
             if (qn) {
                 __syncwarp();
-                flush_queue(a, qaddr, qn, warp_row_pos0, row_stride, lane);
+                flush_queue<kQCap / 32>(g, a.main_words, a.ff_words, a.hits, a.hits_cap, a.counters, qaddr, qn,
+                                              warp_row_pos0, row_stride, lane);
                 qn = 0;
             }
             // lnp is now relative to the next row's start; lnp + 128 is its position in this row
@@ -454,7 +495,7 @@ cudaError_t launch_cfg(const CUtensorMap& map, const FastArgs& fa, int num_sms, 
 template <int L>
 cudaError_t launch_len(int threads, int mode, const CUtensorMap& map, const FastArgs& fa, int num_sms,
                        cudaStream_t st) {
-    if (mode == 1) return launch_cfg<L, 512, 1>(map, fa, num_sms, st);
+    if (mode == 1) return launch_cfg<L, 256, 1>(map, fa, num_sms, st);
     switch (threads) {
         case 256: return launch_cfg<L, 256, 0>(map, fa, num_sms, st);
         case 384: return launch_cfg<L, 384, 0>(map, fa, num_sms, st);
@@ -482,7 +523,7 @@ uint32_t stage1_shift_for_threads(const Geom& g, int threads) {
 
 }  // namespace
 
-int fast_scan_threads() { return g_threads_override ? g_threads_override : 384; }
+int fast_scan_threads() { return g_threads_override ? g_threads_override : 512; }
 
 void set_fast_scan_threads(int t) { g_threads_override = (t == 256 || t == 384 || t == 512) ? t : 0; }
 
@@ -499,7 +540,7 @@ bool fast_scan_supported(const Geom& g, uint64_t n) {
 uint32_t stage1_shift_for(const Geom& g) { return stage1_shift_for_threads(g, fast_scan_threads()); }
 
 cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int mode, int num_sms, cudaStream_t st) {
-    const int threads = mode == 1 ? 512 : fast_scan_threads();
+    const int threads = mode == 1 ? 256 : fast_scan_threads();
     const uint64_t fast_tiles = a.n / kScanTile;  // whole 16 KiB tiles; the rest goes to the generic kernel
     // rows per stream: the largest power of two (<= 16) that still gives every SM several supertiles
     uint32_t rows = 16;
@@ -560,25 +601,15 @@ cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int mode,
     return cudaSuccess;
 }
 
-// Summary of the cache region for the stage-1 test: bit j = OR of cache bits [j << sh, (j + 1) << sh).
-__global__ void k_stage1_summary(const uint32_t* main_words, uint32_t sh, uint32_t* out, uint32_t nwords) {
+// Stage-1 table of T = C >> sh bits for the sparse mode: bit j = OR of the cache bits i with i mod T == j
+// (a fold, so the table index of a window is just h & (T-1)). A window passes the reference test only if
+// its cache bit is set, which sets its table bit: the table rejects only windows the full test rejects.
+__global__ void k_stage1_fold(const uint32_t* main_words, uint32_t sh, uint32_t* out, uint32_t nwords) {
     uint32_t w = blockIdx.x * blockDim.x + threadIdx.x;
     if (w >= nwords) return;
     uint32_t v = 0;
-    for (uint32_t b = 0; b < 32; b++) {
-        const uint64_t lo = ((uint64_t)(w * 32 + b)) << sh, hi = lo + (1ull << sh);
-        bool any = false;
-        for (uint64_t i = lo; i < hi && !any;) {
-            if ((i & 31) == 0 && i + 32 <= hi) {
-                any = main_words[i >> 5] != 0;
-                i += 32;
-            } else {
-                any = (main_words[i >> 5] >> (i & 31)) & 1u;
-                i++;
-            }
-        }
-        v |= (uint32_t)any << b;
-    }
+    const uint32_t folds = 1u << sh;
+    for (uint32_t m = 0; m < folds; m++) v |= main_words[w + m * nwords];
     out[w] = v;
 }
 
@@ -586,7 +617,7 @@ cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, uint32_t* ou
     const uint32_t sh = stage1_shift_for(g);
     const uint32_t nwords = (uint32_t)(((uint64_t)g.cache_bits >> sh) / 32);
     if (sh == 0) return cudaMemcpyAsync(out, main_words, 4ull * nwords, cudaMemcpyDeviceToDevice, st);
-    k_stage1_summary<<<(nwords + 255) / 256, 256, 0, st>>>(main_words, sh, out, nwords);
+    k_stage1_fold<<<(nwords + 255) / 256, 256, 0, st>>>(main_words, sh, out, nwords);
     note_launches(1);
     return cudaGetLastError();
 }
