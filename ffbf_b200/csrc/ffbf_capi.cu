@@ -10,6 +10,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <functional>
 #include <map>
 #include <new>
 #include <string>
@@ -61,14 +62,17 @@ struct ffbf_ctx {
     long long* d_tiles = nullptr;  // 4 arrays of tiles_cap: first, last, prev, next
     uint64_t tiles_cap = 0;
     int scan_path = 0;             // 0 = generic, 1 = fast
-    uint32_t* d_stage1 = nullptr;  // stage-1 table of the tuned scan (cache copy or summary)
+    uint32_t* d_stage1 = nullptr;  // stage-1 table of the tuned scan (cache copy or its fold)
     bool stage1_dirty = true;
-    uint32_t stage1_sh = 0;
+    int stage1_threads = 0;        // CTA size the table was sized for
     unsigned long long* d_popc = nullptr;
     double stage1_fill = 0;
-    int scan_mode = 0;             // 0 sparse, 1 dense (see ffbf_scan_fast.cu)
+    ffbf::FastConfig cfg{512, 0, 0};  // tuned-scan configuration (mode from the stage-1 fill, or the autotuner)
+    bool cfg_tuned = false;
     int force_mode = -1;           // FFBF_SCAN_MODE=0|1 in the environment
     bool force_generic = false;    // FFBF_FORCE_GENERIC_SCAN=1 in the environment
+    ffbf::FastJob* h_job = nullptr;  // pinned staging of a plain scan's job descriptor
+    ffbf::FastJob* d_job = nullptr;
     std::vector<uint64_t> r_hits, r_ls, r_le;
 
     // prune
@@ -91,6 +95,41 @@ struct ffbf_ctx {
     size_t tmp_words = 0;
     uint8_t* d_small = nullptr;  // test_line input
     size_t small_cap = 0;
+};
+
+struct ffbf_batch {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t st = nullptr;
+    std::string err;
+    struct Job {
+        ffbf_ctx* c;
+        const uint8_t* text;
+        size_t len;
+    };
+    // The device buffers and configuration each job's descriptors were built from. A context that has
+    // since grown its hit buffer, reloaded its filter, added patterns or been retuned makes the batch
+    // prepare again before its next launch.
+    struct Key {
+        const void *main, *ff, *hits, *counters, *tiles, *stage1;
+        uint32_t hits_cap;
+        uint64_t tiles_cap;
+        int threads, mode;
+        uint32_t rows;
+        bool operator==(const Key& o) const {
+            return main == o.main && ff == o.ff && hits == o.hits && counters == o.counters && tiles == o.tiles &&
+                   stage1 == o.stage1 && hits_cap == o.hits_cap && tiles_cap == o.tiles_cap && threads == o.threads &&
+                   mode == o.mode && rows == o.rows;
+        }
+    };
+    std::vector<Key> keys;
+    std::vector<Job> jobs;
+    bool prepared = false;
+    std::vector<void*> allocs;
+    uint32_t* d_error = nullptr;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t exec = nullptr;
+    std::function<cudaError_t()> direct;  // the same launches without a graph (FFBF_BATCH_NOGRAPH=1)
 };
 
 namespace {
@@ -247,14 +286,54 @@ void reset_scan(ffbf_ctx* c) {
 
 const uint64_t kInitialHitsCap = 1u << 16;
 
-ffbf_status launch_scan(ffbf_ctx* c) {
-    const uint64_t n = c->text_len;
-    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * sizeof(uint32_t), c->st));
-    if (n == 0) return FFBF_OK;
-    const uint64_t ntiles = (n + ffbf::kScanTile - 1) / ffbf::kScanTile;
+// Makes the tuned scan ready for this context's filter: the stage-1 table for the configured CTA size and,
+// unless the autotuner or the environment fixed it, the probe mode from the table's fill (the shared-memory
+// stage only pays while it rejects most windows).
+ffbf_status prepare_fast(ffbf_ctx* c) {
+    const int sparse_threads = c->cfg.mode == 1 && c->cfg_tuned ? ffbf::fast_scan_threads() : c->cfg.threads;
+    if (c->d_stage1 && c->stage1_threads != sparse_threads) {
+        dfree(c, c->d_stage1);
+        c->stage1_dirty = true;
+    }
+    if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 1));
+    if (!c->h_job) {
+        if (cudaMallocHost(&c->h_job, sizeof(ffbf::FastJob)) != cudaSuccess) {
+            cudaGetLastError();
+            c->h_job = nullptr;
+            return fail(c, FFBF_ENOMEM_HOST, "pinned job descriptor");
+        }
+    }
+    if (!c->d_job) TRY(dalloc_t(c, &c->d_job, 1));
+    if (!c->d_stage1) {
+        TRY(dalloc_t(c, &c->d_stage1, ffbf::stage1_words_for(c->g, sparse_threads)));
+        c->stage1_threads = sparse_threads;
+        c->stage1_dirty = true;
+    }
+    if (c->stage1_dirty) {
+        CUDA_TRY(c, ffbf::build_stage1(c->d_main, c->g, sparse_threads, c->d_stage1, c->st));
+        const uint32_t nw = ffbf::stage1_words_for(c->g, sparse_threads);
+        CUDA_TRY(c, ffbf::popcount_words(c->d_stage1, nw, c->d_popc, c->st));
+        unsigned long long ones = 0;
+        CUDA_TRY(c, cudaMemcpyAsync(&ones, c->d_popc, sizeof ones, cudaMemcpyDeviceToHost, c->st));
+        TRY(sync(c));
+        c->stage1_fill = (double)ones / (32.0 * nw);
+        if (!c->cfg_tuned) c->cfg.mode = c->stage1_fill > 0.3 ? 1 : 0;
+        c->stage1_dirty = false;
+    }
+    if (c->force_mode >= 0) c->cfg.mode = c->force_mode;
+    return FFBF_OK;
+}
+
+ffbf_batch::Key batch_key(const ffbf_ctx* c) {
+    return ffbf_batch::Key{c->d_main, c->d_ff,          c->d_hits,      c->d_counters, c->d_tiles,
+                           c->d_stage1, c->hits_cap,    c->tiles_cap,   c->cfg.threads, c->cfg.mode,
+                           c->cfg.rows};
+}
+
+ffbf::ScanArgs make_scan_args(ffbf_ctx* c) {
     ffbf::ScanArgs a{};
     a.text = c->d_text;
-    a.n = n;
+    a.n = c->text_len;
     a.g = c->g;
     a.main_words = c->d_main;
     a.ff_words = c->d_ff;
@@ -263,42 +342,51 @@ ffbf_status launch_scan(ffbf_ctx* c) {
     a.counters = c->d_counters;
     a.tile_first_nl = c->d_tiles;
     a.tile_last_nl = c->d_tiles + c->tiles_cap;
-    a.ntiles = ntiles;
-    if (ffbf::fast_scan_supported(c->g, n) && !c->force_generic) {
+    a.ntiles = (c->text_len + ffbf::kScanTile - 1) / ffbf::kScanTile;
+    a.tile_begin = 0;
+    a.cache_in_smem = c->g.cache_bits <= ffbf::kSmemCacheMaxBits;
+    return a;
+}
+
+bool use_fast(const ffbf_ctx* c, uint64_t n) { return ffbf::fast_scan_supported(c->g, n) && !c->force_generic; }
+
+ffbf_status launch_scan(ffbf_ctx* c) {
+    const uint64_t n = c->text_len;
+    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * sizeof(uint32_t), c->st));
+    if (n == 0) return FFBF_OK;
+    ffbf::ScanArgs a = make_scan_args(c);
+    if (use_fast(c, n)) {
         c->scan_path = 1;
-        const uint32_t sh = ffbf::stage1_shift_for(c->g);
-        if (c->d_stage1 && c->stage1_sh != sh) {  // the CTA shape changed the table size
-            dfree(c, c->d_stage1);
-            c->stage1_dirty = true;
-        }
-        if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 1));
-        if (!c->d_stage1) {
-            TRY(dalloc_t(c, &c->d_stage1, ffbf::stage1_words_for(c->g)));
-            c->stage1_sh = sh;
-            c->stage1_dirty = true;
-        }
-        if (c->stage1_dirty) {
-            CUDA_TRY(c, ffbf::build_stage1(c->d_main, c->g, c->d_stage1, c->st));
-            // Mode choice: the shared-memory stage only pays while it rejects most windows.
-            const uint32_t nw = ffbf::stage1_words_for(c->g);
-            CUDA_TRY(c, ffbf::popcount_words(c->d_stage1, nw, c->d_popc, c->st));
-            unsigned long long ones = 0;
-            CUDA_TRY(c, cudaMemcpyAsync(&ones, c->d_popc, sizeof ones, cudaMemcpyDeviceToHost, c->st));
-            TRY(sync(c));
-            c->stage1_fill = (double)ones / (32.0 * nw);
-            c->scan_mode = c->stage1_fill > 0.3 ? 1 : 0;
-            c->stage1_dirty = false;
-        }
-        int mode = c->scan_mode;
-        if (c->force_mode >= 0) mode = c->force_mode;
-        CUDA_TRY(c, ffbf::scan_fast(a, c->d_stage1, mode, c->num_sms, c->st));
+        TRY(prepare_fast(c));
+        CUDA_TRY(c, ffbf::scan_fast(a, c->d_stage1, c->cfg, c->num_sms, c->h_job, c->d_job, c->st));
     } else {
         c->scan_path = 0;
-        a.cache_in_smem = c->g.cache_bits <= ffbf::kSmemCacheMaxBits;
-        int grid = ffbf::scan_generic_grid(c->g, a.cache_in_smem, ntiles);
+        int grid = ffbf::scan_generic_grid(c->g, a.cache_in_smem, a.ntiles);
         if (grid <= 0) return fail(c, FFBF_ECUDA, "scan kernel cannot be launched (occupancy query failed)");
         CUDA_TRY(c, ffbf::scan_generic(a, grid, c->st));
     }
+    return FFBF_OK;
+}
+
+// Scan state for a text already on the device, without launching: buffers sized, results reset.
+ffbf_status setup_scan_state(ffbf_ctx* c, const uint8_t* d_text, size_t len) {
+    if (!d_text && len) return fail(c, FFBF_EINVAL, "text pointer is NULL");
+    if (((uintptr_t)d_text & 15) != 0) return fail(c, FFBF_EINVAL, "device text must be 16-byte aligned");
+    reset_scan(c);
+    const uint64_t ntiles = (len + ffbf::kScanTile - 1) / ffbf::kScanTile;
+    if (c->tiles_cap < ntiles) {
+        dfree(c, c->d_tiles);
+        c->tiles_cap = 0;
+        TRY(dalloc_t(c, &c->d_tiles, 4 * ntiles));
+        c->tiles_cap = ntiles;
+    }
+    if (!c->d_hits) {
+        TRY(dalloc_t(c, &c->d_hits, kInitialHitsCap));
+        TRY(dalloc_t(c, &c->d_hitlines, kInitialHitsCap));
+        c->hits_cap = (uint32_t)kInitialHitsCap;
+    }
+    c->d_text = d_text;
+    c->text_len = len;
     return FFBF_OK;
 }
 
@@ -383,6 +471,7 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
     }
     const char* th = getenv("FFBF_SCAN_THREADS");
     if (th) ffbf::set_fast_scan_threads(atoi(th));
+    c->cfg.threads = ffbf::fast_scan_threads();
     const char* fm = getenv("FFBF_SCAN_MODE");
     if (fm && (fm[0] == '0' || fm[0] == '1')) c->force_mode = fm[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");
@@ -398,6 +487,7 @@ void ffbf_destroy(ffbf_ctx* c) {
     for (auto& kv : c->allocs) cudaFree(kv.first);
     c->allocs.clear();
     if (c->h_counters) cudaFreeHost(c->h_counters);
+    if (c->h_job) cudaFreeHost(c->h_job);
     if (c->st) cudaStreamDestroy(c->st);
     cudaGetLastError();
     delete c;
@@ -582,23 +672,7 @@ ffbf_status ffbf_save_filter_file(ffbf_ctx* c, const char* path) {
 
 ffbf_status ffbf_scan_device(ffbf_ctx* c, const uint8_t* d_text, size_t len) {
     TRY(enter(c));
-    if (!d_text && len) return fail(c, FFBF_EINVAL, "text pointer is NULL");
-    if (((uintptr_t)d_text & 15) != 0) return fail(c, FFBF_EINVAL, "device text must be 16-byte aligned");
-    reset_scan(c);
-    const uint64_t ntiles = (len + ffbf::kScanTile - 1) / ffbf::kScanTile;
-    if (c->tiles_cap < ntiles) {
-        dfree(c, c->d_tiles);
-        c->tiles_cap = 0;
-        TRY(dalloc_t(c, &c->d_tiles, 4 * ntiles));
-        c->tiles_cap = ntiles;
-    }
-    if (!c->d_hits) {
-        TRY(dalloc_t(c, &c->d_hits, kInitialHitsCap));
-        TRY(dalloc_t(c, &c->d_hitlines, kInitialHitsCap));
-        c->hits_cap = (uint32_t)kInitialHitsCap;
-    }
-    c->d_text = d_text;
-    c->text_len = len;
+    TRY(setup_scan_state(c, d_text, len));
     TRY(launch_scan(c));
     c->scan_pending = true;
     return FFBF_OK;
@@ -883,6 +957,326 @@ ffbf_status ffbf_get_filters(ffbf_ctx* c, uint8_t* main_bits, uint8_t* ff_bits) 
     if (main_bits) CUDA_TRY(c, cudaMemcpyAsync(main_bits, c->d_main, c->filter_bytes, cudaMemcpyDeviceToHost, c->st));
     if (ff_bits) CUDA_TRY(c, cudaMemcpyAsync(ff_bits, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToHost, c->st));
     return sync(c);
+}
+
+}  // extern "C"
+
+// ---- batched scans ---------------------------------------------------------------------------------------
+namespace {
+
+ffbf_status bfail(ffbf_batch* b, ffbf_status s, const std::string& msg) {
+    b->err = msg;
+    return s;
+}
+
+void batch_release(ffbf_batch* b) {
+    if (b->exec) cudaGraphExecDestroy(b->exec);
+    if (b->graph) cudaGraphDestroy(b->graph);
+    b->exec = nullptr;
+    b->graph = nullptr;
+    for (void* p : b->allocs) cudaFree(p);
+    b->allocs.clear();
+    b->d_error = nullptr;
+    b->prepared = false;
+    b->keys.clear();
+    cudaGetLastError();
+}
+
+template <class T>
+ffbf_status balloc(ffbf_batch* b, T** p, size_t count) {
+    void* v = nullptr;
+    if (cudaMalloc(&v, count * sizeof(T) + 16) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, FFBF_ENOMEM_DEVICE, "batch table allocation failed");
+    }
+    b->allocs.push_back(v);
+    *p = static_cast<T*>(v);
+    return FFBF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ffbf_status ffbf_batch_create(int device, ffbf_batch** out) {
+    if (!out) return FFBF_EINVAL;
+    *out = nullptr;
+    ffbf_batch* b = new (std::nothrow) ffbf_batch();
+    if (!b) return FFBF_ENOMEM_HOST;
+    b->device = device;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        delete b;
+        return FFBF_ECUDA;
+    }
+    *out = b;
+    return FFBF_OK;
+}
+
+void ffbf_batch_destroy(ffbf_batch* b) {
+    if (!b) return;
+    cudaSetDevice(b->device);
+    if (b->st) cudaStreamSynchronize(b->st);
+    batch_release(b);
+    if (b->st) cudaStreamDestroy(b->st);
+    delete b;
+}
+
+const char* ffbf_batch_last_error(const ffbf_batch* b) { return b ? b->err.c_str() : "null batch"; }
+
+void* ffbf_batch_stream(ffbf_batch* b) { return b ? (void*)b->st : nullptr; }
+
+ffbf_status ffbf_batch_add(ffbf_batch* b, ffbf_ctx* c, const uint8_t* d_text, size_t len) {
+    if (!b || !c) return FFBF_EINVAL;
+    if (c->device != b->device) return bfail(b, FFBF_EINVAL, "context and batch are on different devices");
+    if (((uintptr_t)d_text & 15) != 0 || (!d_text && len)) return bfail(b, FFBF_EINVAL, "device text must be 16-byte aligned");
+    for (auto& j : b->jobs)
+        if (j.c == c) return bfail(b, FFBF_EINVAL, "a context may appear only once in a batch");
+    if (b->prepared) batch_release(b);
+    b->jobs.push_back({c, d_text, len});
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
+    if (!b) return FFBF_EINVAL;
+    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, FFBF_ECUDA, "cudaSetDevice failed");
+    batch_release(b);
+    struct Group {
+        uint32_t len;
+        ffbf::FastConfig cfg;
+        std::vector<std::pair<uint64_t, ffbf::FastJob>> jobs;  // (bytes, descriptor)
+    };
+    std::vector<Group> groups;
+    std::vector<ffbf::ScanArgs> args;
+    std::vector<uint2> tail;
+    std::vector<uint32_t*> counters;
+    for (uint32_t i = 0; i < b->jobs.size(); i++) {
+        ffbf_ctx* c = b->jobs[i].c;
+        ffbf_status s = enter(c);
+        if (s == FFBF_OK) s = setup_scan_state(c, b->jobs[i].text, b->jobs[i].len);
+        if (s != FFBF_OK) return bfail(b, s, std::string("job setup: ") + c->err);
+        const ffbf::ScanArgs a = make_scan_args(c);
+        args.push_back(a);
+        counters.push_back(c->d_counters);
+        uint64_t covered = 0;
+        if (use_fast(c, a.n)) {
+            if ((s = prepare_fast(c)) != FFBF_OK) return bfail(b, s, std::string("job filter: ") + c->err);
+            const ffbf::FastConfig cfg = c->cfg;
+            const int threads = ffbf::config_threads(cfg);
+            const uint32_t rows = cfg.rows ? cfg.rows : ffbf::fast_rows(a.n, threads, b->num_sms, true);
+            ffbf::FastJob fj;
+            cudaError_t e;
+            covered = ffbf::fill_fast_job(a, c->d_stage1, cfg, rows, &fj, &e);
+            if (e != cudaSuccess) return bfail(b, FFBF_ECUDA, "tensor map encoding failed");
+            if (fj.n_supertiles) {
+                Group* gp = nullptr;
+                for (auto& g : groups)
+                    if (g.len == c->g.len && g.cfg.mode == cfg.mode && ffbf::config_threads(g.cfg) == threads) gp = &g;
+                if (!gp) {
+                    groups.push_back(Group{c->g.len, cfg, {}});
+                    gp = &groups.back();
+                }
+                gp->jobs.push_back({covered, fj});
+            }
+        }
+        for (uint64_t t = covered / ffbf::kScanTile; t < a.ntiles; t++) tail.push_back(make_uint2(i, (uint32_t)t));
+        if (cudaStreamSynchronize(c->st) != cudaSuccess) return bfail(b, FFBF_ECUDA, "context stream failed");
+        c->scan_pending = true;
+        b->keys.push_back(batch_key(c));
+    }
+    // descriptors: groups contiguous, largest jobs first within a group
+    std::vector<ffbf::FastJob> fast;
+    struct Launch {
+        uint32_t len;
+        ffbf::FastConfig cfg;
+        size_t off;
+        uint32_t n_jobs, n_items, max_s1;
+    };
+    std::vector<Launch> launches;
+    for (auto& g : groups) {
+        std::stable_sort(g.jobs.begin(), g.jobs.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
+        Launch L{g.len, g.cfg, fast.size(), (uint32_t)g.jobs.size(), 0, 0};
+        for (auto& jb : g.jobs) {
+            jb.second.item_begin = L.n_items;
+            L.n_items += jb.second.n_supertiles;
+            L.max_s1 = std::max(L.max_s1, jb.second.stage1_nwords);
+            fast.push_back(jb.second);
+        }
+        launches.push_back(L);
+    }
+    ffbf::FastJob* d_fast = nullptr;
+    ffbf::ScanArgs* d_args = nullptr;
+    uint2* d_tail = nullptr;
+    uint32_t** d_counters = nullptr;
+    TRY(balloc(b, &d_fast, fast.size() + 1));
+    TRY(balloc(b, &d_args, args.size() + 1));
+    TRY(balloc(b, &d_tail, tail.size() + 1));
+    TRY(balloc(b, &d_counters, counters.size() + 1));
+    TRY(balloc(b, &b->d_error, 1));
+    if ((fast.size() && cudaMemcpy(d_fast, fast.data(), fast.size() * sizeof(ffbf::FastJob), cudaMemcpyHostToDevice)) ||
+        (args.size() && cudaMemcpy(d_args, args.data(), args.size() * sizeof(ffbf::ScanArgs), cudaMemcpyHostToDevice)) ||
+        (tail.size() && cudaMemcpy(d_tail, tail.data(), tail.size() * sizeof(uint2), cudaMemcpyHostToDevice)) ||
+        (counters.size() &&
+         cudaMemcpy(d_counters, counters.data(), counters.size() * sizeof(uint32_t*), cudaMemcpyHostToDevice)) ||
+        cudaMemset(b->d_error, 0, sizeof(uint32_t)))
+        return bfail(b, FFBF_ECUDA, "batch table upload failed");
+    const char* dbg = getenv("FFBF_BATCH_DEBUG");
+    if (dbg && dbg[0] == '1') {
+        // diagnostic: the same launches, uncaptured, each checked before the next
+        auto check = [&](cudaError_t e, const char* what) -> ffbf_status {
+            if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+            if (e != cudaSuccess) {
+                cudaGetLastError();
+                return bfail(b, FFBF_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
+            }
+            return FFBF_OK;
+        };
+        TRY(check(ffbf::zero_counters(d_counters, (uint32_t)counters.size(), b->st), "zero_counters"));
+        for (const Launch& L : launches) {
+            char what[96];
+            snprintf(what, sizeof what, "tuned launch len %u threads %d mode %d jobs %u items %u", L.len,
+                     ffbf::config_threads(L.cfg), L.cfg.mode, L.n_jobs, L.n_items);
+            TRY(check(ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error,
+                                             b->num_sms, b->st),
+                      what));
+        }
+        TRY(check(ffbf::scan_generic_multi(d_args, d_tail, (uint32_t)tail.size(), b->num_sms, b->st), "generic tail"));
+    }
+    {
+        const uint32_t n_counters = (uint32_t)counters.size(), n_tail = (uint32_t)tail.size();
+        b->direct = [=]() {
+            cudaError_t e = ffbf::zero_counters(d_counters, n_counters, b->st);
+            for (const Launch& L : launches) {
+                if (e != cudaSuccess) break;
+                e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error,
+                                           b->num_sms, b->st);
+            }
+            if (e == cudaSuccess) e = ffbf::scan_generic_multi(d_args, d_tail, n_tail, b->num_sms, b->st);
+            return e;
+        };
+    }
+    // one graph: zero the jobs' counters, one tuned launch per group, one generic launch for all tail tiles
+    if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
+        return bfail(b, FFBF_ECUDA, "stream capture failed to start");
+    cudaError_t e = ffbf::zero_counters(d_counters, (uint32_t)counters.size(), b->st);
+    for (const Launch& L : launches) {
+        if (e != cudaSuccess) break;
+        e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error, b->num_sms,
+                                   b->st);
+    }
+    if (e == cudaSuccess) e = ffbf::scan_generic_multi(d_args, d_tail, (uint32_t)tail.size(), b->num_sms, b->st);
+    cudaError_t e2 = cudaStreamEndCapture(b->st, &b->graph);
+    if (e != cudaSuccess || e2 != cudaSuccess || cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, FFBF_ECUDA, std::string("batch graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
+    }
+    b->prepared = true;
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_batch_launch(ffbf_batch* b) {
+    if (!b) return FFBF_EINVAL;
+    bool stale = !b->prepared || b->keys.size() != b->jobs.size();
+    for (size_t i = 0; i < b->jobs.size() && !stale; i++)
+        stale = !(batch_key(b->jobs[i].c) == b->keys[i]) ||
+                (use_fast(b->jobs[i].c, b->jobs[i].len) && b->jobs[i].c->stage1_dirty);
+    if (stale) TRY(ffbf_batch_prepare(b));
+    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, FFBF_ECUDA, "cudaSetDevice failed");
+    for (auto& j : b->jobs) {
+        reset_scan(j.c);
+        j.c->d_text = j.text;
+        j.c->text_len = j.len;
+        j.c->scan_pending = true;
+    }
+    const char* ng = getenv("FFBF_BATCH_NOGRAPH");
+    if (ng && ng[0] == '1') {
+        if (b->direct() != cudaSuccess) {
+            cudaGetLastError();
+            return bfail(b, FFBF_ECUDA, "direct batch launch failed");
+        }
+        return FFBF_OK;
+    }
+    if (cudaGraphLaunch(b->exec, b->st) != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, FFBF_ECUDA, "graph launch failed");
+    }
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_batch_wait(ffbf_batch* b) {
+    if (!b) return FFBF_EINVAL;
+    cudaError_t e = cudaSetDevice(b->device);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        return bfail(b, FFBF_ECUDA, std::string("batch execution failed: ") + cudaGetErrorString(e));
+    }
+    uint32_t flag = 0;
+    if (b->d_error && cudaMemcpy(&flag, b->d_error, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
+        return bfail(b, FFBF_ECUDA, "error flag read failed");
+    if (flag) {
+        char buf[96];
+        snprintf(buf, sizeof buf, "batched scan error flags 0x%x (4: a bounded wait gave up; others: self-checks)", flag);
+        return bfail(b, (flag & 4u) ? FFBF_ETIMEOUT : FFBF_ECUDA, buf);
+    }
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len, int* threads, int* mode) {
+    TRY(enter(c));
+    if (!d_text || ((uintptr_t)d_text & 15)) return fail(c, FFBF_EINVAL, "device text must be 16-byte aligned");
+    if (!use_fast(c, sample_len)) return fail(c, FFBF_EINVAL, "the tuned scan does not cover this geometry or size");
+    // keep the feed-forward filter: the trial scans set bits in it
+    uint32_t* saved = nullptr;
+    TRY(dalloc_t(c, &saved, c->filter_bytes / 4));
+    CUDA_TRY(c, cudaMemcpyAsync(saved, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
+    const ffbf::FastConfig cands[] = {{512, 0, 0}, {384, 0, 0}, {256, 0, 0}, {256, 1, 0}};
+    ffbf::FastConfig best = c->cfg;
+    float best_ms = 1e30f;
+    cudaEvent_t e0, e1;
+    cudaEventCreate(&e0);
+    cudaEventCreate(&e1);
+    const int saved_force = c->force_mode;
+    c->force_mode = -1;
+    ffbf_status s = FFBF_OK;
+    for (const auto& cand : cands) {
+        c->cfg = cand;
+        c->cfg_tuned = true;
+        ffbf::set_fast_scan_threads(cand.mode == 0 ? cand.threads : 0);
+        if ((s = setup_scan_state(c, d_text, sample_len)) != FFBF_OK) break;
+        float ms = 1e30f;
+        for (int rep = 0; rep < 3 && s == FFBF_OK; rep++) {
+            cudaEventRecord(e0, c->st);
+            s = launch_scan(c);
+            cudaEventRecord(e1, c->st);
+            if (cudaEventSynchronize(e1) != cudaSuccess) s = fail(c, FFBF_ECUDA, "autotune timing failed");
+            float t = 0;
+            cudaEventElapsedTime(&t, e0, e1);
+            if (rep > 0) ms = std::min(ms, t);  // the first run also builds the stage-1 table
+        }
+        if (s != FFBF_OK) break;
+        if (ms < best_ms) {
+            best_ms = ms;
+            best = cand;
+        }
+    }
+    c->force_mode = saved_force;
+    ffbf::set_fast_scan_threads(best.mode == 0 ? best.threads : 0);
+    c->cfg = best;
+    c->cfg_tuned = true;
+    reset_scan(c);
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    if (s == FFBF_OK) {
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_ff, saved, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
+        s = sync(c);
+    }
+    dfree(c, saved);
+    if (s == FFBF_OK) s = prepare_fast(c);
+    if (threads) *threads = ffbf::config_threads(best);
+    if (mode) *mode = best.mode;
+    return s;
 }
 
 }  // extern "C"

@@ -207,6 +207,83 @@ size_t scan_smem_bytes(int cache_in_smem, const Geom& g) {
     return b;
 }
 
+// One 16 KiB tile of the generic scan (window ends [tile*T, tile*T + T)). The caller provides the shared
+// S-box copy, the tile newline accumulator, the padded staging buffer and the cache-region words to probe
+// (shared-memory copy or the global filter).
+__device__ __forceinline__ void generic_tile(const ScanArgs& a, uint64_t tile, const uint64_t* s_sbox, long long* s_nl,
+                                             uint8_t* s_text, const uint32_t* cache_words) {
+    const Geom g = a.g;
+    const uint32_t L = g.len;
+    const int tid = threadIdx.x;
+    __syncthreads();
+    const long long t0 = (long long)(tile * kScanTile);
+    for (int q = tid; q < (kScanTile + kHalo) / 4; q += kScanThreads) {
+        long long p = t0 - kHalo + 4LL * q;
+        uint32_t v;
+        if (p >= 0 && p + 4 <= (long long)a.n) {
+            v = __ldg(reinterpret_cast<const uint32_t*>(a.text + p));
+        } else {
+            v = 0;
+            for (int j = 0; j < 4; j++) {
+                long long pj = p + j;
+                uint32_t b = (pj < 0 || pj >= (long long)a.n) ? 0x0Au : a.text[pj];
+                v |= b << (8 * j);
+            }
+        }
+        *reinterpret_cast<uint32_t*>(s_text + pad_idx(4 * q)) = v;
+    }
+    if (tid == 0) {
+        s_nl[0] = LLONG_MAX;
+        s_nl[1] = -1;
+    }
+    __syncthreads();
+
+    const long long seg0 = t0 + (long long)tid * kScanSeg;
+    long long my_first = LLONG_MAX, my_last = -1;
+    if (seg0 < (long long)a.n) {
+        const long long seg1 = min(seg0 + kScanSeg, (long long)a.n);
+        // staged byte of text position p: s_text[pad_idx(p - (t0 - kHalo))]
+        const long long off = kHalo - t0;
+        uint64_t h = 0;
+        uint32_t run = 0;
+        for (long long p = seg0 - L; p < seg0; p++) {
+            uint32_t c = s_text[pad_idx((uint32_t)(p + off))];
+            h = rol64(h, 1) ^ s_sbox[c];
+            run = c == 0x0Au ? 0u : min(run + 1u, L);
+        }
+        for (long long p = seg0; p < seg1; p++) {
+            uint32_t c = s_text[pad_idx((uint32_t)(p + off))];
+            uint32_t co = s_text[pad_idx((uint32_t)(p - L + off))];
+            h = rol64(h, 1) ^ s_sbox[c] ^ rol64(s_sbox[co], L);
+            if (c == 0x0Au) {
+                run = 0;
+                if (my_first == LLONG_MAX) my_first = p;
+                my_last = p;
+                continue;
+            }
+            run = min(run + 1u, L);
+            if (run < L) continue;
+            bool hit = true;
+            for (uint32_t i = 0; i < g.k && hit; i++) {
+                uint32_t b = bit_index<1>(g, h, i);
+                hit = test_bit(i < g.s ? cache_words : a.main_words, b);
+            }
+            if (hit) {
+                set_all<2>(g, a.ff_words, h);
+                uint32_t slot = atomicAdd(a.counters + CNT_HITS, 1u);
+                if (slot < a.hits_cap) a.hits[slot] = HitRec{(uint64_t)(p + 1 - L), h};
+            }
+        }
+    }
+    if (my_first != LLONG_MAX) atomicMin(s_nl + 0, my_first);
+    if (my_last >= 0) atomicMax(s_nl + 1, my_last);
+    __syncthreads();
+    if (tid == 0) {
+        a.tile_first_nl[tile] = s_nl[0];
+        a.tile_last_nl[tile] = s_nl[1];
+    }
+}
+
 __global__ void __launch_bounds__(kScanThreads) k_scan_generic(ScanArgs a) {
     extern __shared__ __align__(16) uint8_t smem[];
     uint64_t* s_sbox = reinterpret_cast<uint64_t*>(smem);
@@ -214,84 +291,58 @@ __global__ void __launch_bounds__(kScanThreads) k_scan_generic(ScanArgs a) {
     uint8_t* s_text = smem + 2048 + 16;
     const uint32_t text_bytes = (pad_idx(kScanTile + kHalo) + 16 + 15) & ~15u;
     uint32_t* s_cache = reinterpret_cast<uint32_t*>(s_text + text_bytes);
-
-    const Geom g = a.g;
-    const uint32_t L = g.len;
     const int tid = threadIdx.x;
     for (int i = tid; i < 256; i += kScanThreads) s_sbox[i] = c_sbox[(i & 0x80) ? 0 : i];
     if (a.cache_in_smem)
-        for (uint32_t w = tid; w < g.cache_bits / 32; w += kScanThreads) s_cache[w] = a.main_words[w];
+        for (uint32_t w = tid; w < a.g.cache_bits / 32; w += kScanThreads) s_cache[w] = a.main_words[w];
     const uint32_t* cache_words = a.cache_in_smem ? s_cache : a.main_words;
+    for (uint64_t tile = a.tile_begin + blockIdx.x; tile < a.ntiles; tile += gridDim.x)
+        generic_tile(a, tile, s_sbox, s_nl, s_text, cache_words);
+}
 
-    for (uint64_t tile = a.tile_begin + blockIdx.x; tile < a.ntiles; tile += gridDim.x) {
-        __syncthreads();
-        const long long t0 = (long long)(tile * kScanTile);
-        for (int q = tid; q < (kScanTile + kHalo) / 4; q += kScanThreads) {
-            long long p = t0 - kHalo + 4LL * q;
-            uint32_t v;
-            if (p >= 0 && p + 4 <= (long long)a.n) {
-                v = __ldg(reinterpret_cast<const uint32_t*>(a.text + p));
-            } else {
-                v = 0;
-                for (int j = 0; j < 4; j++) {
-                    long long pj = p + j;
-                    uint32_t b = (pj < 0 || pj >= (long long)a.n) ? 0x0Au : a.text[pj];
-                    v |= b << (8 * j);
-                }
-            }
-            *reinterpret_cast<uint32_t*>(s_text + pad_idx(4 * q)) = v;
+// Generic scan over tiles of many jobs: item i is tile items[i].y of job items[i].x. Probes the global filter.
+__global__ void __launch_bounds__(kScanThreads) k_scan_generic_multi(const ScanArgs* jobs, const uint2* items,
+                                                                     uint32_t n_items) {
+    extern __shared__ __align__(16) uint8_t smem[];
+    uint64_t* s_sbox = reinterpret_cast<uint64_t*>(smem);
+    long long* s_nl = reinterpret_cast<long long*>(smem + 2048);
+    uint8_t* s_text = smem + 2048 + 16;
+    for (int i = threadIdx.x; i < 256; i += kScanThreads) s_sbox[i] = c_sbox[(i & 0x80) ? 0 : i];
+    for (uint32_t i = blockIdx.x; i < n_items; i += gridDim.x) {
+        const uint2 it = items[i];
+        const ScanArgs a = jobs[it.x];
+        if (it.y >= a.ntiles) {  // self-check: skip a tile outside the job's text
+            if (threadIdx.x == 0) atomicOr(a.counters + CNT_ERROR, 0x1000u);
+            continue;
         }
-        if (tid == 0) {
-            s_nl[0] = LLONG_MAX;
-            s_nl[1] = -1;
-        }
-        __syncthreads();
-
-        const long long seg0 = t0 + (long long)tid * kScanSeg;
-        long long my_first = LLONG_MAX, my_last = -1;
-        if (seg0 < (long long)a.n) {
-            const long long seg1 = min(seg0 + kScanSeg, (long long)a.n);
-            // staged byte of text position p: s_text[pad_idx(p - (t0 - kHalo))]
-            const long long off = kHalo - t0;
-            uint64_t h = 0;
-            uint32_t run = 0;
-            for (long long p = seg0 - L; p < seg0; p++) {
-                uint32_t c = s_text[pad_idx((uint32_t)(p + off))];
-                h = rol64(h, 1) ^ s_sbox[c];
-                run = c == 0x0Au ? 0u : min(run + 1u, L);
-            }
-            for (long long p = seg0; p < seg1; p++) {
-                uint32_t c = s_text[pad_idx((uint32_t)(p + off))];
-                uint32_t co = s_text[pad_idx((uint32_t)(p - L + off))];
-                h = rol64(h, 1) ^ s_sbox[c] ^ rol64(s_sbox[co], L);
-                if (c == 0x0Au) {
-                    run = 0;
-                    if (my_first == LLONG_MAX) my_first = p;
-                    my_last = p;
-                    continue;
-                }
-                run = min(run + 1u, L);
-                if (run < L) continue;
-                bool hit = true;
-                for (uint32_t i = 0; i < g.k && hit; i++) {
-                    uint32_t b = bit_index<1>(g, h, i);
-                    hit = test_bit(i < g.s ? cache_words : a.main_words, b);
-                }
-                if (hit) {
-                    set_all<2>(g, a.ff_words, h);
-                    uint32_t slot = atomicAdd(a.counters + CNT_HITS, 1u);
-                    if (slot < a.hits_cap) a.hits[slot] = HitRec{(uint64_t)(p + 1 - L), h};
-                }
-            }
-        }
-        if (my_first != LLONG_MAX) atomicMin(s_nl + 0, my_first);
-        if (my_last >= 0) atomicMax(s_nl + 1, my_last);
-        __syncthreads();
-        if (tid == 0) {
-            a.tile_first_nl[tile] = s_nl[0];
-            a.tile_last_nl[tile] = s_nl[1];
-        }
+        generic_tile(a, it.y, s_sbox, s_nl, s_text, a.main_words);
     }
+}
+
+cudaError_t scan_generic_multi(const ScanArgs* d_jobs, const uint2* d_items, uint32_t n_items, int num_sms,
+                               cudaStream_t st) {
+    if (!n_items) return cudaSuccess;
+    const Geom none{};
+    const size_t smem = scan_smem_bytes(0, none);
+    cudaError_t e = cudaFuncSetAttribute(k_scan_generic_multi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    const uint32_t grid = n_items < (uint32_t)(4 * num_sms) ? n_items : (uint32_t)(4 * num_sms);
+    k_scan_generic_multi<<<grid, kScanThreads, smem, st>>>(d_jobs, d_items, n_items);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
+// Zeroes the counters of every job of a batch.
+__global__ void k_zero_counters(uint32_t* const* ptrs, uint32_t n) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n * CNT_WORDS) ptrs[i / CNT_WORDS][i % CNT_WORDS] = 0;
+}
+
+cudaError_t zero_counters(uint32_t* const* d_ptrs, uint32_t n, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    k_zero_counters<<<(n * CNT_WORDS + 255) / 256, 256, 0, st>>>(d_ptrs, n);
+    note_launches(1);
+    return cudaGetLastError();
 }
 
 int scan_generic_grid(const Geom& g, int cache_in_smem, uint64_t ntiles) {

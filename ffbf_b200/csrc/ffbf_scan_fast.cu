@@ -31,6 +31,7 @@
 #include <cudaTypedefs.h>
 
 #include <climits>
+#include <cstring>
 
 #include "ffbf_scan_fast.cuh"
 
@@ -44,24 +45,6 @@ constexpr int kQueueCap = 64;            // candidates per warp queue
 constexpr int kQueueBytes = kQueueCap * 16;
 constexpr uint32_t kWaitLimit = 1u << 24;
 constexpr size_t kSmemLimit = 232448;    // opt-in shared memory per block on sm_100
-
-struct FastArgs {
-    uint64_t n_streams;      // streams covered by the tensor map
-    uint32_t rows;           // rows per stream
-    uint32_t n_supertiles;   // ceil(n_streams / THREADS)
-    uint32_t streams_per_tile_log2;  // log2(16384 / (rows * 128))
-    Geom g;
-    const uint32_t* main_words;
-    uint32_t* ff_words;
-    const uint32_t* stage1_words;  // cache region copy or its summary (global), copied into smem
-    uint32_t stage1_nwords;
-    uint32_t stage1_shift;         // the table holds C >> shift bits (0: exact copy of the cache region)
-    HitRec* hits;
-    uint32_t hits_cap;
-    uint32_t* counters;
-    long long* tile_first_nl;
-    long long* tile_last_nl;
-};
 
 __device__ __forceinline__ uint32_t smem_u32(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
 
@@ -178,6 +161,10 @@ __device__ __noinline__ void flush_queue(const Geom g, const uint32_t* __restric
         if (!((v[t] >> (bi[t] & 31)) & 1u)) continue;
         if (!full_check_from(g, main_words, h, e[t].w + 1)) continue;
         const uint32_t owner = e[t].x >> 8, p = e[t].x & 0xFFu;
+        if (owner >= 32 || p >= 128) {
+            atomicOr(counters + CNT_ERROR, 0x400u);
+            continue;
+        }
         const uint64_t start = warp_row_pos0 + owner * row_stride + p + 1 - g.len;
         set_all<2>(g, ff_words, h);
         const uint32_t slot = atomicAdd(counters + CNT_HITS, 1u);
@@ -186,13 +173,20 @@ __device__ __noinline__ void flush_queue(const Geom g, const uint32_t* __restric
     __syncwarp();
 }
 
+// Work items. Job j owns items [item_begin_j, item_begin_{j+1}), one per supertile of THREADS streams; CTA b
+// takes items b, b + gridDim.x, ... Each item is one TMA load of the streams' halo rows followed by `rows`
+// row loads. Thread 0 issues load k+1 while the CTA consumes load k and records in meta[] which job, item
+// and row each buffer holds.
+//
 // MODE 0 (sparse filters): stage 1 in shared memory, candidates queued per byte.
-// MODE 1 (dense filters, where a shared-memory summary would pass most windows): the exact h1 probe is a
-// global load issued for every valid window and consumed kRing bytes later from a register ring, so the
-// L2 latency overlaps the hashing of the next windows; windows whose h1 bit is set go to the queue.
+// MODE 1 (dense filters, where a shared-memory table would pass most windows): the exact probes of the
+// first two index functions are global loads issued per valid window and consumed kRing bytes later from
+// register rings, so L2 latency overlaps the hashing of the next windows; only windows whose two probed bits
+// are set go to the queue.
 template <int L, int THREADS, int MODE>
-__global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant__ CUtensorMap tmap,
-                                                          const __grid_constant__ FastArgs a) {
+__global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
+                                                          uint32_t n_items, uint32_t max_s1_words,
+                                                          uint32_t* __restrict__ error_flag) {
     constexpr int kStageBytes = THREADS * kRowBytes;
     constexpr int kQCap = MODE == 0 ? kQueueCap : 2 * kQueueCap;
     constexpr int kQBytes = kQCap * 16;
@@ -202,12 +196,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
     uint8_t* smem = smem_raw + (base - raw);
-    // layout: [stage 0][stage 1][S tables][mbarriers (128 B)][warp queues][stage-1 table]
+    // layout: [stage 0][stage 1][S tables][mbarriers, meta (128 B)][warp queues][stage-1 table]
     const uint32_t stage0 = base;
     const uint32_t tab = base + 2 * kStageBytes;
     const uint32_t bar0 = tab + kTabBytes, bar1 = bar0 + 8;
+    int* meta = reinterpret_cast<int*>(smem + 2 * kStageBytes + kTabBytes + 16);  // [buf][4]: job, item, row, valid
     const uint32_t queues = bar0 + 128;
     const uint32_t s1 = queues + (THREADS / 32) * kQBytes;
+    uint32_t* s1p = reinterpret_cast<uint32_t*>(smem + (s1 - base));
     __shared__ int s_abort;
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -217,44 +213,56 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
             const int c = i >> 4;
             tp[i] = c_sbox[(c & 0x80) ? 0 : c];
         }
-        uint32_t* sp = reinterpret_cast<uint32_t*>(smem + (s1 - base));
-        for (uint32_t i = tid; i < a.stage1_nwords; i += THREADS) sp[i] = a.stage1_words[i];
     }
+    // load sequencer, run by thread 0: the next load is row nr (-1: halo) of item ni, which belongs to job nj
+    uint32_t ni = blockIdx.x, nj = 0;
+    int nr = -1;
+    auto issue = [&](uint32_t k) {
+        int* m = meta + 4 * (k & 1);
+        if (ni >= n_items) {
+            m[3] = 0;
+            return;
+        }
+        while (nj + 1 < n_jobs && __ldg(&jobs[nj + 1].item_begin) <= ni) nj++;
+        const FastJob* J = jobs + nj;
+        const uint32_t R = __ldg(&J->rows);
+        const uint32_t st = ni - __ldg(&J->item_begin);
+        const int y = nr < 0 ? (int)R - 1 : nr;
+        const int z = (int)(st * THREADS) + (nr < 0 ? -1 : 0);
+        const uint32_t bar = (k & 1) ? bar1 : bar0;
+        const uint32_t dst = stage0 + (k & 1) * kStageBytes;
+        m[0] = (int)nj;
+        m[1] = (int)st;
+        m[2] = nr;
+        m[3] = 1;
+        mbar_expect_tx(bar, kStageBytes);
+        for (int b = 0; b < THREADS / kBox; b++)
+            tma_load_3d(dst + b * kBox * kRowBytes, &J->tmap, 0, y, z + b * kBox, bar);
+        if (++nr == (int)R) {
+            nr = -1;
+            ni += gridDim.x;
+        }
+    };
     if (tid == 0) {
         s_abort = 0;
         mbar_init(bar0, 1);
         mbar_init(bar1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+        issue(0);
     }
     __syncthreads();
 
-    const Geom g = a.g;
-    const uint32_t R = a.rows;
-    const uint32_t per_st = R + 1;  // halo load + R row loads
-    uint32_t my_st = 0;
-    if (blockIdx.x < a.n_supertiles) my_st = (a.n_supertiles - 1 - blockIdx.x) / gridDim.x + 1;
-    const uint32_t total = my_st * per_st;
     const uint32_t lane_tab = tab + (uint32_t)(lane & 15) * 8u;  // entry c of this lane's copy: + c * 128
-    const uint32_t cmask = g.cache_mask;
-    // stage-1 table of T = C >> shift bits, folded modulo T: the byte offset of bit (h & (T-1))'s word is
-    // (h >> 3) & s1_bmask
-    const uint32_t s1_bmask = (((cmask >> a.stage1_shift) >> 3) & ~3u);
-    const bool two = g.s > 1;
     const uint32_t qaddr = queues + (uint32_t)warp * kQBytes;
     const unsigned lt_mask = (1u << lane) - 1u;
 
-    auto issue = [&](uint32_t k) {
-        const uint32_t st = blockIdx.x + (k / per_st) * gridDim.x;
-        const int r = (int)(k % per_st) - 1;
-        const int y = r < 0 ? (int)R - 1 : r;
-        const int z = (int)(st * THREADS) + (r < 0 ? -1 : 0);
-        const uint32_t bar = (k & 1) ? bar1 : bar0;
-        const uint32_t dst = stage0 + (k & 1) * kStageBytes;
-        mbar_expect_tx(bar, kStageBytes);
-        for (int b = 0; b < THREADS / kBox; b++) tma_load_3d(dst + b * kBox * kRowBytes, &tmap, 0, y, z + b * kBox, bar);
-    };
-
-    if (tid == 0 && total > 0) issue(0);
+    // the current job's parameters (reloaded when the job changes)
+    int cur_job = -1;
+    Geom g{};
+    uint32_t R = 0, cmask = 0, s1_bmask = 0, p2_mask = 0, p2_add = 0, s1_first = 0, spt_log2 = 0;
+    bool two = false;
+    uint64_t n_streams = 0;
+    const FastJob* J = jobs;
 
     int qn = 0;  // warp-uniform queue fill
     uint64_t warp_row_pos0 = 0, row_stride = 0;
@@ -264,6 +272,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
         if (m) {
             if (pass) {
                 const uint32_t slot = (uint32_t)qn + __popc(m & lt_mask);
+                if (slot >= (uint32_t)kQCap) atomicOr(error_flag, 0x800u);
+                else
                 asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(qaddr + 16u * slot),
                              "r"(pos | ((uint32_t)lane << 8)), "r"(ql), "r"(qh), "r"(first)
                              : "memory");
@@ -271,8 +281,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
             qn += __popc(m);
             if (qn > kQCap - 32) {
                 __syncwarp();
-                flush_queue<kQCap / 32>(g, a.main_words, a.ff_words, a.hits, a.hits_cap, a.counters, qaddr, qn,
-                                              warp_row_pos0, row_stride, lane);
+                flush_queue<kQCap / 32>(g, J->main_words, J->ff_words, J->hits, J->hits_cap, J->counters, qaddr, qn,
+                                        warp_row_pos0, row_stride, lane);
                 qn = 0;
             }
         }
@@ -283,42 +293,72 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
     uint32_t ring_v[kR], ring_l[kR], ring_h[kR], ring2_v[kR], ring2_l[kR], ring2_h[kR];
 #pragma unroll
     for (int q = 0; q < kR; q++) ring_v[q] = ring_l[q] = ring_h[q] = ring2_v[q] = ring2_l[q] = ring2_h[q] = 0;
-    // second probe's index function (getHashValue case 1): cache region when S > 1, else external region
-    const uint32_t p2_mask = two ? cmask : g.ext_mask, p2_add = two ? 0u : g.cache_bits;
-    // sparse mode: the stage-1 probes are exact when the table is the cache region itself
-    const uint32_t s1_first = a.stage1_shift == 0 ? (two ? 2u : 1u) : 0u;
 
     uint32_t hl = 0, hh = 0;
     int lnp = -1000;  // last '\n' relative to the current row start
     long long first_nl = LLONG_MAX, last_nl = -1;
     uint32_t prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
-    for (uint32_t k = 0; k < total; k++) {
-        if (tid == 0 && k + 1 < total) issue(k + 1);
+    for (uint32_t k = 0;; k++) {
+        const int* m = meta + 4 * (k & 1);
+        if (!m[3]) break;
+        const int job = m[0];
+        const uint32_t st = (uint32_t)m[1];
+        const int r = m[2];
+        if (tid == 0) issue(k + 1);
         const uint32_t bar = (k & 1) ? bar1 : bar0;
         const uint32_t parity = (k >> 1) & 1u;
         uint32_t it = 0;
         while (!mbar_try_wait(bar, parity)) {
             if (++it >= kWaitLimit) {
-                atomicOr(a.counters + CNT_ERROR, 4u);
+                atomicOr(error_flag, 4u);
                 s_abort = 1;
                 break;
             }
         }
         if (s_abort) {
             // Give the load issued for k + 1 a bounded chance to land before this CTA's shared memory goes away.
-            if (tid == 0 && k + 1 < total) {
+            if (tid == 0 && meta[4 * ((k + 1) & 1) + 3]) {
                 const uint32_t nb = ((k + 1) & 1) ? bar1 : bar0;
                 for (uint32_t j = 0; j < kWaitLimit && !mbar_try_wait(nb, ((k + 1) >> 1) & 1u); j++) {
                 }
             }
             break;
         }
+        if (job != cur_job) {
+            cur_job = job;
+            J = jobs + job;
+            g = J->g;
+            R = J->rows;
+            n_streams = J->n_streams;
+            spt_log2 = J->streams_per_tile_log2;
+            cmask = g.cache_mask;
+            two = g.s > 1;
+            // stage-1 table of T = C >> shift bits, folded modulo T: the byte offset of bit (h & (T-1))'s
+            // word is (h >> 3) & s1_bmask
+            s1_bmask = (((cmask >> J->stage1_shift) >> 3) & ~3u);
+            // second probe's index function (getHashValue case 1): cache region when S > 1, else external
+            p2_mask = two ? cmask : g.ext_mask;
+            p2_add = two ? 0u : g.cache_bits;
+            // sparse mode: the stage-1 probes are exact when the table is the cache region itself
+            s1_first = J->stage1_shift == 0 ? (two ? 2u : 1u) : 0u;
+            if constexpr (MODE == 0) {
+                const uint32_t nw = J->stage1_nwords;
+                const uint32_t* src = J->stage1_words;
+                for (uint32_t i = tid; i < nw; i += THREADS) s1p[i] = src[i];
+                __syncthreads();
+            }
+        }
 
-        const uint32_t st = blockIdx.x + (k / per_st) * gridDim.x;
-        const int r = (int)(k % per_st) - 1;
+        // self-checks: a bad descriptor or sequencing records a code and skips the work
+        if ((uint32_t)job >= n_jobs || st >= J->n_supertiles || r < -1 || r >= (int)R ||
+            (MODE == 0 && J->stage1_nwords > max_s1_words)) {
+            if (tid == 0) atomicOr(error_flag, 0x100u);
+            __syncthreads();
+            continue;
+        }
         const uint64_t z = (uint64_t)st * THREADS + tid;
-        const bool active = z < a.n_streams;
+        const bool active = z < n_streams;
         const uint8_t* row = smem + (k & 1) * kStageBytes + tid * kRowBytes;
         const int sw = tid & 7;
 
@@ -334,10 +374,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
 #pragma unroll
             for (int j = 0; j < 32; j++) {
                 const uint32_t c = byte_at(prev[j >> 2], j & 3);
-                const uint2 s = lds64(lane_tab + c * 128u);
+                const uint2 sv = lds64(lane_tab + c * 128u);
                 uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
-                nl ^= s.x;
-                nh ^= s.y;
+                nl ^= sv.x;
+                nh ^= sv.y;
                 if (j >= L) {
                     const uint32_t co = byte_at(prev[(j - L) >> 2], (j - L) & 3);
                     const uint2 o = lds64(lane_tab + co * 128u);
@@ -375,13 +415,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
                     uint32_t co;
                     if (j >= L) co = byte_at(cur[(j - L) >> 2], (j - L) & 3);
                     else co = byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
-                    const uint2 s = lds64(lane_tab + c * 128u);
+                    const uint2 sv = lds64(lane_tab + c * 128u);
                     const uint2 o = lds64(lane_tab + co * 128u);
                     uint32_t rl, rh;
                     rol_pair<L>(o.x, o.y, rl, rh);
                     const uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
-                    hl = nl ^ s.x ^ rl;
-                    hh = nh ^ s.y ^ rh;
+                    hl = nl ^ sv.x ^ rl;
+                    hh = nh ^ sv.y ^ rh;
                     if (c == 0x0Au) lnp = j;
                     if constexpr (MODE == 0) {
                         const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
@@ -400,18 +440,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
                         const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], ring_l[slot]) & 1u) != 0;
                         ring2_l[slot] = ring_l[slot];
                         ring2_h[slot] = ring_h[slot];
-                        ring2_v[slot] = ldg_if(a.main_words + (((ring_h[slot] & p2_mask) + p2_add) >> 5), pass1);
+                        ring2_v[slot] = ldg_if(J->main_words + (((ring_h[slot] & p2_mask) + p2_add) >> 5), pass1);
                         const bool valid = active && (j - lnp >= L);
                         ring_l[slot] = hl;
                         ring_h[slot] = hh;
-                        ring_v[slot] = ldg_if(a.main_words + ((hl & cmask) >> 5), valid);
+                        ring_v[slot] = ldg_if(J->main_words + ((hl & cmask) >> 5), valid);
                     }
                 }
                 if (lnp != lnp_blk && row_first < 0 && first_nl == LLONG_MAX) {
-                    for (int k = 0; k < 8 && row_first < 0; k++) {
-                        const uint32_t t = cur[k] ^ 0x0A0A0A0Au;
+                    for (int q = 0; q < 8 && row_first < 0; q++) {
+                        const uint32_t t = cur[q] ^ 0x0A0A0A0Au;
                         const uint32_t zb = ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
-                        if (zb) row_first = 32 * b + 4 * k + (__ffs(zb) - 1) / 8;
+                        if (zb) row_first = 32 * b + 4 * q + (__ffs(zb) - 1) / 8;
                     }
                 }
                 lnp -= 32;
@@ -433,8 +473,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
             }
             if (qn) {
                 __syncwarp();
-                flush_queue<kQCap / 32>(g, a.main_words, a.ff_words, a.hits, a.hits_cap, a.counters, qaddr, qn,
-                                              warp_row_pos0, row_stride, lane);
+                flush_queue<kQCap / 32>(g, J->main_words, J->ff_words, J->hits, J->hits_cap, J->counters, qaddr, qn,
+                                        warp_row_pos0, row_stride, lane);
                 qn = 0;
             }
             // lnp is now relative to the next row's start; lnp + 128 is its position in this row
@@ -446,15 +486,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const __grid_constant_
             if ((uint32_t)r == R - 1) {
                 // per-16 KiB-tile newline summary: reduce over the lanes whose streams share the tile
                 long long f = active ? first_nl : LLONG_MAX, l = active ? last_nl : -1;
-                const int G = 1 << a.streams_per_tile_log2;
+                const int G = 1 << spt_log2;
                 for (int o = 1; o < G; o <<= 1) {
                     f = min(f, __shfl_xor_sync(0xffffffffu, f, o));
                     l = max(l, __shfl_xor_sync(0xffffffffu, l, o));
                 }
                 if (active && (lane & (G - 1)) == 0) {
-                    const uint64_t tile = z >> a.streams_per_tile_log2;
-                    a.tile_first_nl[tile] = f;
-                    a.tile_last_nl[tile] = l;
+                    const uint64_t tile = z >> spt_log2;
+                    if (tile < J->n_tiles) {
+                        J->tile_first_nl[tile] = f;
+                        J->tile_last_nl[tile] = l;
+                    } else {
+                        atomicOr(error_flag, 0x200u);
+                    }
                 }
             }
         }
@@ -481,25 +525,27 @@ constexpr size_t fixed_smem() {
 }
 
 template <int L, int THREADS, int MODE>
-cudaError_t launch_cfg(const CUtensorMap& map, const FastArgs& fa, int num_sms, cudaStream_t st) {
-    const size_t smem = fixed_smem<THREADS, MODE>() + 4 * (size_t)fa.stage1_nwords;
+cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items, uint32_t max_s1_words,
+                       uint32_t* d_error, int num_sms, cudaStream_t st) {
+    const size_t smem = fixed_smem<THREADS, MODE>() + (MODE == 0 ? 4 * (size_t)max_s1_words : 0);
     cudaError_t e =
         cudaFuncSetAttribute(k_scan_fast<L, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int grid = (int)(fa.n_supertiles < (uint32_t)num_sms ? fa.n_supertiles : (uint32_t)num_sms);
-    k_scan_fast<L, THREADS, MODE><<<grid, THREADS, smem, st>>>(map, fa);
+    const int grid = (int)(n_items < (uint32_t)num_sms ? n_items : (uint32_t)num_sms);
+    if (grid == 0) return cudaSuccess;
+    k_scan_fast<L, THREADS, MODE><<<grid, THREADS, smem, st>>>(d_jobs, n_jobs, n_items, max_s1_words, d_error);
     note_launches(1);
     return cudaGetLastError();
 }
 
 template <int L>
-cudaError_t launch_len(int threads, int mode, const CUtensorMap& map, const FastArgs& fa, int num_sms,
-                       cudaStream_t st) {
-    if (mode == 1) return launch_cfg<L, 256, 1>(map, fa, num_sms, st);
-    switch (threads) {
-        case 256: return launch_cfg<L, 256, 0>(map, fa, num_sms, st);
-        case 384: return launch_cfg<L, 384, 0>(map, fa, num_sms, st);
-        default: return launch_cfg<L, 512, 0>(map, fa, num_sms, st);
+cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
+                       uint32_t max_s1_words, uint32_t* d_error, int num_sms, cudaStream_t st) {
+    if (cfg.mode == 1) return launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_error, num_sms, st);
+    switch (cfg.threads) {
+        case 256: return launch_cfg<L, 256, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        case 384: return launch_cfg<L, 384, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        default: return launch_cfg<L, 512, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
     }
 }
 
@@ -512,14 +558,6 @@ size_t fixed_smem_for(int threads) {
 }
 
 int g_threads_override = 0;
-
-// Largest power-of-two stage-1 table (in bits, <= C) that fits beside the fixed shared-memory layout.
-uint32_t stage1_shift_for_threads(const Geom& g, int threads) {
-    const size_t room = kSmemLimit - fixed_smem_for(threads) - 64;
-    uint32_t sh = 0;
-    while (((uint64_t)g.cache_bits >> sh) / 8 > room) sh++;
-    return sh;
-}
 
 }  // namespace
 
@@ -537,68 +575,113 @@ bool fast_scan_supported(const Geom& g, uint64_t n) {
     return encoder() != nullptr;
 }
 
-uint32_t stage1_shift_for(const Geom& g) { return stage1_shift_for_threads(g, fast_scan_threads()); }
+// Largest power-of-two stage-1 table (in bits, <= C) that fits beside the fixed shared-memory layout.
+uint32_t stage1_shift_for(const Geom& g, int threads) {
+    const size_t room = kSmemLimit - fixed_smem_for(threads) - 64;
+    uint32_t sh = 0;
+    while (((uint64_t)g.cache_bits >> sh) / 8 > room) sh++;
+    return sh;
+}
 
-cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int mode, int num_sms, cudaStream_t st) {
-    const int threads = mode == 1 ? 256 : fast_scan_threads();
-    const uint64_t fast_tiles = a.n / kScanTile;  // whole 16 KiB tiles; the rest goes to the generic kernel
-    // rows per stream: the largest power of two (<= 16) that still gives every SM several supertiles
+uint32_t stage1_words_for(const Geom& g, int threads) {
+    return (uint32_t)(((uint64_t)g.cache_bits >> stage1_shift_for(g, threads)) / 32);
+}
+
+int config_threads(const FastConfig& cfg) { return cfg.mode == 1 ? 256 : cfg.threads; }
+
+uint32_t fast_rows(uint64_t n, int threads, int num_sms, bool batch) {
+    const uint64_t tiles_bytes = n / kScanTile * kScanTile;
     uint32_t rows = 16;
-    while (rows > 4 && fast_tiles * kScanTile / ((uint64_t)rows * kRowBytes * threads) < 4ull * num_sms) rows >>= 1;
+    if (batch) {
+        // in a batch other jobs fill the GPU: the largest tile this job still fills four times over
+        while (rows > 4 && tiles_bytes < 4ull * rows * kRowBytes * threads) rows >>= 1;
+    } else {
+        // alone: enough supertiles for several per SM
+        while (rows > 4 && tiles_bytes / ((uint64_t)rows * kRowBytes * threads) < 4ull * num_sms) rows >>= 1;
+    }
+    return rows;
+}
+
+uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const FastConfig& cfg, uint32_t rows,
+                       FastJob* job, cudaError_t* err) {
+    *err = cudaSuccess;
+    const int threads = config_threads(cfg);
+    const uint64_t fast_tiles = a.n / kScanTile;  // whole 16 KiB tiles; the rest goes to the generic kernel
     const uint64_t slen = (uint64_t)rows * kRowBytes;
     const uint64_t n_streams = fast_tiles * kScanTile / slen;
-    FastArgs fa{};
-    fa.n_streams = n_streams;
-    fa.rows = rows;
-    fa.n_supertiles = (uint32_t)((n_streams + threads - 1) / threads);
+    memset(job, 0, sizeof *job);
+    job->n_streams = n_streams;
+    job->rows = rows;
+    job->n_supertiles = (uint32_t)((n_streams + threads - 1) / threads);
     uint32_t spt = (uint32_t)(kScanTile / slen), lg = 0;
     while ((1u << lg) < spt) lg++;
-    fa.streams_per_tile_log2 = lg;
-    fa.g = a.g;
-    fa.main_words = a.main_words;
-    fa.ff_words = a.ff_words;
-    fa.stage1_words = stage1_words;
-    fa.stage1_shift = mode == 1 ? 0 : stage1_shift_for_threads(a.g, threads);
-    fa.stage1_nwords = mode == 1 ? 0 : (uint32_t)(((uint64_t)a.g.cache_bits >> fa.stage1_shift) / 32);
-    fa.hits = a.hits;
-    fa.hits_cap = a.hits_cap;
-    fa.counters = a.counters;
-    fa.tile_first_nl = a.tile_first_nl;
-    fa.tile_last_nl = a.tile_last_nl;
-
+    job->streams_per_tile_log2 = lg;
+    job->g = a.g;
+    job->main_words = a.main_words;
+    job->ff_words = a.ff_words;
+    job->stage1_words = stage1_words;
+    job->stage1_shift = cfg.mode == 1 ? 0 : stage1_shift_for(a.g, threads);
+    job->stage1_nwords = cfg.mode == 1 ? 0 : (uint32_t)(((uint64_t)a.g.cache_bits >> job->stage1_shift) / 32);
+    job->hits = a.hits;
+    job->hits_cap = a.hits_cap;
+    job->counters = a.counters;
+    job->tile_first_nl = a.tile_first_nl;
+    job->tile_last_nl = a.tile_last_nl;
+    job->n_tiles = a.ntiles;
     if (n_streams > 0) {
-        CUtensorMap map;
         const uint32_t box_streams = threads > 256 ? (uint32_t)threads / 2 : (uint32_t)threads;
         cuuint64_t dims[3] = {(cuuint64_t)kRowBytes, (cuuint64_t)rows, (cuuint64_t)n_streams};
         cuuint64_t strides[2] = {(cuuint64_t)kRowBytes, (cuuint64_t)slen};
         cuuint32_t box[3] = {(cuuint32_t)kRowBytes, 1u, box_streams};
         cuuint32_t estr[3] = {1u, 1u, 1u};
-        CUresult cr = encoder()(&map, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)a.text, dims, strides, box, estr,
+        CUresult cr = encoder()(&job->tmap, CU_TENSOR_MAP_DATA_TYPE_UINT8, 3, (void*)a.text, dims, strides, box, estr,
                                 CU_TENSOR_MAP_INTERLEAVE_NONE, CU_TENSOR_MAP_SWIZZLE_128B,
                                 CU_TENSOR_MAP_L2_PROMOTION_L2_256B, CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE);
-        if (cr != CUDA_SUCCESS) return cudaErrorInvalidValue;
-        cudaError_t e;
-        switch (a.g.len) {
-            case 16: e = launch_len<16>(threads, mode, map, fa, num_sms, st); break;
-            case 19: e = launch_len<19>(threads, mode, map, fa, num_sms, st); break;
-            case 20: e = launch_len<20>(threads, mode, map, fa, num_sms, st); break;
-            case 24: e = launch_len<24>(threads, mode, map, fa, num_sms, st); break;
-            case 32: e = launch_len<32>(threads, mode, map, fa, num_sms, st); break;
-            default: return cudaErrorInvalidValue;
-        }
+        if (cr != CUDA_SUCCESS) *err = cudaErrorInvalidValue;
+    }
+    return fast_tiles * kScanTile;
+}
+
+cudaError_t launch_fast_jobs(uint32_t len, const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs,
+                             uint32_t n_items, uint32_t max_s1_words, uint32_t* d_error, int num_sms,
+                             cudaStream_t st) {
+    switch (len) {
+        case 16: return launch_len<16>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        case 19: return launch_len<19>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        case 20: return launch_len<20>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        case 24: return launch_len<24>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        case 32: return launch_len<32>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        default: return cudaErrorInvalidValue;
+    }
+}
+
+cudaError_t scan_tail(const ScanArgs& a, uint64_t covered, cudaStream_t st) {
+    const uint64_t ntiles = (a.n + kScanTile - 1) / kScanTile;
+    const uint64_t first = covered / kScanTile;
+    if (first >= ntiles) return cudaSuccess;
+    ScanArgs t = a;
+    t.tile_begin = first;
+    t.cache_in_smem = a.g.cache_bits <= kSmemCacheMaxBits;
+    const int grid = scan_generic_grid(a.g, t.cache_in_smem, ntiles - first);
+    if (grid <= 0) return cudaErrorInvalidConfiguration;
+    return scan_generic(t, grid, st);
+}
+
+cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, const FastConfig& cfg, int num_sms,
+                      FastJob* h_job, FastJob* d_job, cudaStream_t st) {
+    const int threads = config_threads(cfg);
+    const uint32_t rows = cfg.rows ? cfg.rows : fast_rows(a.n, threads, num_sms, false);
+    cudaError_t e;
+    const uint64_t covered = fill_fast_job(a, stage1_words, cfg, rows, h_job, &e);
+    if (e != cudaSuccess) return e;
+    if (h_job->n_supertiles) {
+        e = cudaMemcpyAsync(d_job, h_job, sizeof(FastJob), cudaMemcpyHostToDevice, st);
+        if (e != cudaSuccess) return e;
+        e = launch_fast_jobs(a.g.len, cfg, d_job, 1, h_job->n_supertiles, h_job->stage1_nwords,
+                             a.counters + CNT_ERROR, num_sms, st);
         if (e != cudaSuccess) return e;
     }
-    // the partial last tile through the generic kernel
-    const uint64_t ntiles = (a.n + kScanTile - 1) / kScanTile;
-    if (fast_tiles < ntiles) {
-        ScanArgs t = a;
-        t.tile_begin = fast_tiles;
-        t.cache_in_smem = a.g.cache_bits <= kSmemCacheMaxBits;
-        const int grid = scan_generic_grid(a.g, t.cache_in_smem, ntiles - fast_tiles);
-        if (grid <= 0) return cudaErrorInvalidConfiguration;
-        return scan_generic(t, grid, st);
-    }
-    return cudaSuccess;
+    return scan_tail(a, covered, st);
 }
 
 // Stage-1 table of T = C >> sh bits for the sparse mode: bit j = OR of the cache bits i with i mod T == j
@@ -613,16 +696,14 @@ __global__ void k_stage1_fold(const uint32_t* main_words, uint32_t sh, uint32_t*
     out[w] = v;
 }
 
-cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, uint32_t* out, cudaStream_t st) {
-    const uint32_t sh = stage1_shift_for(g);
+cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, int threads, uint32_t* out, cudaStream_t st) {
+    const uint32_t sh = stage1_shift_for(g, threads);
     const uint32_t nwords = (uint32_t)(((uint64_t)g.cache_bits >> sh) / 32);
     if (sh == 0) return cudaMemcpyAsync(out, main_words, 4ull * nwords, cudaMemcpyDeviceToDevice, st);
     k_stage1_fold<<<(nwords + 255) / 256, 256, 0, st>>>(main_words, sh, out, nwords);
     note_launches(1);
     return cudaGetLastError();
 }
-
-uint32_t stage1_words_for(const Geom& g) { return (uint32_t)(((uint64_t)g.cache_bits >> stage1_shift_for(g)) / 32); }
 
 }  // namespace ffbf
 

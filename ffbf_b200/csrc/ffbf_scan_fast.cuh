@@ -1,30 +1,75 @@
-// ffbf_scan_fast.cuh -- the tuned sm_100a scan (see ffbf_scan_fast.cu).
+// ffbf_scan_fast.cuh -- the tuned sm_100a scan (see ffbf_scan_fast.cu): job descriptors, configuration, launch.
 #pragma once
+#include <cuda.h>
+
 #include "ffbf_kernels.cuh"
 
 namespace ffbf {
 
+// One scan job of the tuned kernel (a text, its filter, its outputs). Jobs live in device memory; a plain
+// scan is a batch of one. The tensor map is the first member (64-byte alignment).
+struct alignas(64) FastJob {
+    CUtensorMap tmap;        // the text as {128 bytes, rows, n_streams}
+    uint64_t n_streams;      // streams covered by the tensor map
+    uint32_t rows;           // rows per stream (tile size: a supertile is THREADS * rows * 128 bytes)
+    uint32_t n_supertiles;   // ceil(n_streams / THREADS)
+    uint32_t item_begin;     // first work item of this job; the next job's item_begin ends it
+    uint32_t streams_per_tile_log2;  // log2(16384 / (rows * 128))
+    Geom g;
+    const uint32_t* main_words;
+    uint32_t* ff_words;
+    const uint32_t* stage1_words;  // sparse mode: cache region copy or its fold (global), copied into smem
+    uint32_t stage1_nwords;
+    uint32_t stage1_shift;         // the table holds C >> shift bits (0: exact copy of the cache region)
+    HitRec* hits;
+    uint32_t hits_cap;
+    uint32_t pad;
+    uint32_t* counters;
+    long long* tile_first_nl;
+    long long* tile_last_nl;
+    uint64_t n_tiles;  // 16 KiB tiles of the text (bounds the newline summary writes)
+};
+
+// How a job is scanned: CTA size (256/384/512; the dense mode always uses 256), probe mode (0: sparse,
+// shared-memory stage 1; 1: dense, pipelined L2 probes), rows per stream (0: chosen from the text size).
+struct FastConfig {
+    int threads;
+    int mode;
+    uint32_t rows;
+};
+
 // True when the tuned kernel handles this geometry and text size; otherwise the generic scan runs.
 bool fast_scan_supported(const Geom& g, uint64_t n);
 
-// Same contract as scan_generic over tiles [0, ntiles): sets feed-forward bits, appends hits, fills the
-// per-tile newline summaries (kScanTile granularity) that resolve_lines reads. Whole 16 KiB tiles run in
-// the tuned kernel, a partial last tile in the generic one. stage1_words is the device buffer filled by
-// build_stage1 for the current main filter.
-// mode 0: sparse filters (shared-memory stage 1); mode 1: dense filters (pipelined exact h1 probe in L2).
-cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, int mode, int num_sms, cudaStream_t st);
+// Default CTA size of the sparse mode; anything other than 256/384/512 restores it.
+int fast_scan_threads();
+void set_fast_scan_threads(int threads);
+int config_threads(const FastConfig& cfg);
+
+// Stage-1 table of the sparse mode for a CTA size: a copy of the cache region when it fits in the shared
+// memory left over, otherwise its fold to C >> shift bits.
+uint32_t stage1_shift_for(const Geom& g, int threads);
+uint32_t stage1_words_for(const Geom& g, int threads);
+cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, int threads, uint32_t* out, cudaStream_t st);
+
+// Rows per stream for a text of n bytes, alone on the GPU or in a batch.
+uint32_t fast_rows(uint64_t n, int threads, int num_sms, bool batch);
+
+// Fills *job (host memory) for the whole 16 KiB tiles of a.text and returns the bytes it covers; the
+// caller sets item_begin. scan_tail runs the generic kernel over the tiles from `covered` on.
+uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const FastConfig& cfg, uint32_t rows,
+                       FastJob* job, cudaError_t* err);
+cudaError_t scan_tail(const ScanArgs& a, uint64_t covered, cudaStream_t st);
+
+// One launch of the tuned kernel over n_jobs device-resident jobs sharing LEN and configuration.
+cudaError_t launch_fast_jobs(uint32_t len, const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs,
+                             uint32_t n_items, uint32_t max_s1_words, uint32_t* d_error, int num_sms, cudaStream_t st);
+
+// A plain scan: one job (h_job pinned host staging, d_job device copy) plus the generic tail.
+cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, const FastConfig& cfg, int num_sms,
+                      FastJob* h_job, FastJob* d_job, cudaStream_t st);
 
 // Number of set bits in n words, written to *d_out (device).
 cudaError_t popcount_words(const uint32_t* w, uint32_t n, unsigned long long* d_out, cudaStream_t st);
-
-// Stage-1 table of the tuned scan: a copy of the cache region when it fits in shared memory, otherwise
-// its OR-summary. stage1_words_for gives its size in 32-bit words.
-uint32_t stage1_words_for(const Geom& g);
-uint32_t stage1_shift_for(const Geom& g);
-
-// Threads per CTA of the tuned scan (256, 384 or 512); anything else restores the default.
-int fast_scan_threads();
-void set_fast_scan_threads(int threads);
-cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, uint32_t* out, cudaStream_t st);
 
 }  // namespace ffbf

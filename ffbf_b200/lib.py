@@ -35,7 +35,9 @@ EXPORTED = [
     "ffbf_save_filter", "ffbf_load_filter_file", "ffbf_save_filter_file", "ffbf_scan", "ffbf_scan_device",
     "ffbf_scan_collect", "ffbf_format_lines", "ffbf_prune", "ffbf_format_pruned", "ffbf_verify",
     "ffbf_test_line", "ffbf_clear_ff", "ffbf_get_filters", "ffbf_filter_bytes", "ffbf_free", "ffbf_format_spans",
-    "ffbf_stream", "ffbf_kernel_launches", "ffbf_scan_static",
+    "ffbf_stream", "ffbf_kernel_launches", "ffbf_scan_static", "ffbf_batch_create", "ffbf_batch_add",
+    "ffbf_batch_prepare", "ffbf_batch_launch", "ffbf_batch_wait", "ffbf_batch_stream", "ffbf_batch_last_error",
+    "ffbf_batch_destroy", "ffbf_autotune",
 ]
 
 
@@ -124,6 +126,15 @@ def load_library(path=LIB_PATH):
         "ffbf_kernel_launches": (ctypes.c_uint64, []),
         "ffbf_scan_static": (ctypes.c_int, [P(Params), vp, vp, vp, ctypes.c_uint64, vp, vp, vp,
                                             P(ctypes.c_uint32), vp]),
+        "ffbf_batch_create": (ctypes.c_int, [ctypes.c_int, P(vp)]),
+        "ffbf_batch_add": (ctypes.c_int, [vp, vp, vp, sz]),
+        "ffbf_batch_prepare": (ctypes.c_int, [vp]),
+        "ffbf_batch_launch": (ctypes.c_int, [vp]),
+        "ffbf_batch_wait": (ctypes.c_int, [vp]),
+        "ffbf_batch_stream": (vp, [vp]),
+        "ffbf_batch_last_error": (ctypes.c_char_p, [vp]),
+        "ffbf_batch_destroy": (None, [vp]),
+        "ffbf_autotune": (ctypes.c_int, [vp, vp, sz, P(ctypes.c_int), P(ctypes.c_int)]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -314,6 +325,12 @@ class Filter:
         self._check(self._lib.ffbf_test_line(self._h, p, n, ctypes.byref(hit)))
         return bool(hit.value)
 
+    def autotune(self, dev_ptr, n):
+        """Times the tuned scan's configurations on n device bytes; keeps the fastest. Returns (threads, mode)."""
+        t, m = ctypes.c_int(), ctypes.c_int()
+        self._check(self._lib.ffbf_autotune(self._h, ctypes.c_void_p(dev_ptr), n, ctypes.byref(t), ctypes.byref(m)))
+        return t.value, m.value
+
     def clear_ff(self):
         self._check(self._lib.ffbf_clear_ff(self._h))
 
@@ -324,3 +341,54 @@ class Filter:
         self._check(self._lib.ffbf_get_filters(self._h, main.ctypes.data_as(ctypes.c_void_p),
                                                ff.ctypes.data_as(ctypes.c_void_p)))
         return main, ff
+
+
+class Batch:
+    """Many (Filter, device text) scan jobs in one graph launch (ffbf_batch_*)."""
+
+    def __init__(self, device=0):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        st = self._lib.ffbf_batch_create(device, ctypes.byref(h))
+        if st != 0:
+            raise FFBFError(st, "ffbf_batch_create failed")
+        self._h = h
+        self._filters = []
+
+    def _check(self, st):
+        if st != 0:
+            raise FFBFError(st, self._lib.ffbf_batch_last_error(self._h).decode(errors="replace"))
+
+    def add(self, filt, dev_ptr, n):
+        self._check(self._lib.ffbf_batch_add(self._h, filt._h, ctypes.c_void_p(dev_ptr), n))
+        self._filters.append(filt)
+
+    def prepare(self):
+        self._check(self._lib.ffbf_batch_prepare(self._h))
+
+    def launch(self):
+        self._check(self._lib.ffbf_batch_launch(self._h))
+
+    def wait(self):
+        self._check(self._lib.ffbf_batch_wait(self._h))
+
+    @property
+    def stream(self):
+        return int(self._lib.ffbf_batch_stream(self._h) or 0)
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ffbf_batch_destroy(self._h)
+            self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass

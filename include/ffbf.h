@@ -170,6 +170,34 @@ ffbf_status ffbf_verify(ffbf_ctx* ctx, ffbf_matches* out);
  * reference, '\n' inside `line` is hashed as an ordinary byte, and lines shorter than LEN give 0. */
 ffbf_status ffbf_test_line(ffbf_ctx* ctx, const uint8_t* line, size_t len, int* hit);
 
+/* ---- Batched scans ------------------------------------------------------------------------------------
+ * Many (context, device text) jobs scanned together. The reference processes one text per run; batching
+ * is this library's answer to many small jobs, which one launch per job leaves mostly idle: the tuned
+ * kernel walks a combined list of all jobs' tiles, one persistent launch per group of jobs sharing LEN and
+ * CTA shape, and all of a batch's launches are captured in one CUDA graph. Per job the tile size and the
+ * filter placement (shared-memory stage 1 or pipelined L2 probes) are chosen by ffbf_autotune's rules.
+ *
+ * Each job writes into its own context as ffbf_scan_device would: after ffbf_batch_wait, call
+ * ffbf_scan_collect (then ffbf_prune / ffbf_verify) on each context. A context may appear once per batch,
+ * must not be used by other calls between ffbf_batch_prepare and ffbf_batch_wait, and its texts must stay
+ * valid until then. ffbf_batch_launch may be called repeatedly (each launch zeroes the jobs' hit counters;
+ * feed-forward filters accumulate, as for repeated scans). */
+typedef struct ffbf_batch ffbf_batch;
+ffbf_status ffbf_batch_create(int device, ffbf_batch** out);
+ffbf_status ffbf_batch_add(ffbf_batch* b, ffbf_ctx* ctx, const uint8_t* d_text, size_t len);
+ffbf_status ffbf_batch_prepare(ffbf_batch* b);   /* job tables, stage-1 tables, graph capture */
+ffbf_status ffbf_batch_launch(ffbf_batch* b);    /* one graph launch on the batch's stream */
+ffbf_status ffbf_batch_wait(ffbf_batch* b);
+void* ffbf_batch_stream(ffbf_batch* b);
+const char* ffbf_batch_last_error(const ffbf_batch* b);
+void ffbf_batch_destroy(ffbf_batch* b);
+
+/* Autotuner: times the tuned scan's configurations (CTA size, shared-memory vs L2 filter placement) on the
+ * first `sample_len` bytes of a device text with this context's filter, keeps the fastest for later scans
+ * of the context, and reports it (threads, mode: 0 shared-memory stage, 1 pipelined L2 probes). The
+ * feed-forward filter is left unchanged. Without it, the placement follows the stage-1 table's fill. */
+ffbf_status ffbf_autotune(ffbf_ctx* ctx, const uint8_t* d_text, size_t sample_len, int* threads, int* mode);
+
 /* Zeroes the feed-forward filter (a fresh reverseBitvector, ffbf.cpp:107). Enqueued on the context's
  * stream; later calls on the context see it done. */
 ffbf_status ffbf_clear_ff(ffbf_ctx* ctx);
