@@ -44,7 +44,10 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["scale", "plain", "binary"], default="scale")
+    ap.add_argument("--workload", choices=["scale", "plain", "binary", "batched"], default="scale")
+    ap.add_argument("--batch-jobs", type=int, default=512, help="jobs of the batched workload")
+    ap.add_argument("--batch-max-text", type=int, default=256 << 20, help="largest job text of the batched workload")
+    ap.add_argument("--no-batched", action="store_true", help="skip the batched leg of the default run")
     ap.add_argument("--text-bytes", type=int, default=0, help="override the workload's text size")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (default: min(steps, 5))")
@@ -265,6 +268,153 @@ def main_reference(args):
     return 0
 
 
+# ---- batched form: 512 uneven jobs in one graph launch vs plain per-job launches ------------------------
+def ff_digest(f):
+    """A 64-bit digest of a filter's feed-forward bit array (copied to the host)."""
+    import ctypes
+    ff = np.zeros(f.filter_bytes, dtype=np.uint8)
+    f._check(f._lib.ffbf_get_filters(f._h, None, ff.ctypes.data_as(ctypes.c_void_p)))
+    w = ff.view(np.uint64)
+    idx = np.arange(w.size, dtype=np.uint64)
+    return int(np.bitwise_xor.reduce(w * (idx * np.uint64(0x9E3779B97F4A7C15) | np.uint64(1)))) ^ int(w.sum())
+
+
+def run_batched(args, local):
+    """Scans every job of the batched workload in three forms and checks that they agree bit for bit.
+
+    Forms: `batched` = ffbf_batch_launch (one graph: counters reset, one persistent tuned launch per
+    (LEN, configuration) group with a work queue over all its jobs' items, one generic launch for every
+    job's ragged tail); `plain_serial` = ffbf_scan_device per job, each waited for before the next (one
+    job per launch, as a caller of the plain API runs them); `plain_streams` = ffbf_scan_device for all jobs
+    back to back, each on its own context stream, then one wait (the plain API's best case).
+    Texts are device resident in all forms; all are timed by the host clock between device-idle points,
+    the batched form also by CUDA events on the batch's stream.
+    """
+    from concurrent.futures import ThreadPoolExecutor
+
+    import torch
+
+    import ffbf_b200
+    from ffbf_b200 import Batch, Filter
+    from ffbf_b200 import datagen as dg
+
+    dev = torch.device("cuda", local)
+    jobs = dg.batched(n_jobs=args.batch_jobs, text_hi=args.batch_max_text, seed=args.seed)
+    t_gen = time.perf_counter()
+    with ThreadPoolExecutor(min(32, os.cpu_count() or 1)) as ex:
+        pats = list(ex.map(lambda w: w.patterns(w.seed), jobs))
+    offs, total = [], 0
+    for w in jobs:
+        offs.append(total)
+        total += (w.text_bytes + 255) // 256 * 256
+    host = torch.empty(total, dtype=torch.uint8, pin_memory=True)
+    hv = host.numpy()
+    for w, pb, o in zip(jobs, pats, offs):
+        w.text(w.seed, pb, out=hv[o:o + w.text_bytes])
+    d_all = torch.empty(total, dtype=torch.uint8, device=dev)
+    d_all.copy_(host)
+    filters = []
+    for w, pb in zip(jobs, pats):
+        f = Filter(w.params, device=local)
+        f.add_patterns(pb)
+        filters.append(f)
+    torch.cuda.synchronize()
+    gen_s = time.perf_counter() - t_gen
+    base = d_all.data_ptr()
+    nbytes = sum(w.text_bytes for w in jobs)
+
+    def plain_serial():
+        for f, w, o in zip(filters, jobs, offs):
+            f.process_device(base + o, w.text_bytes)
+            torch.cuda.ExternalStream(f.stream, device=dev).synchronize()
+
+    def plain_streams():
+        for f, w, o in zip(filters, jobs, offs):
+            f.process_device(base + o, w.text_bytes)
+        for f in filters:
+            torch.cuda.ExternalStream(f.stream, device=dev).synchronize()
+
+    b = Batch(local)
+    for f, w, o in zip(filters, jobs, offs):
+        b.add(f, base + o, w.text_bytes)
+    t0 = time.perf_counter()
+    b.prepare()
+    prepare_s = time.perf_counter() - t0
+
+    def batched():
+        b.launch()
+        b.wait()
+
+    def timed(fn):
+        for _ in range(args.warmup):
+            fn()
+        torch.cuda.synchronize()
+        launches0 = ffbf_b200.kernel_launches()
+        ts = []
+        for _ in range(args.steps):
+            t = time.perf_counter()
+            fn()
+            ts.append(time.perf_counter() - t)
+        return statistics.median(ts), (ffbf_b200.kernel_launches() - launches0) // max(args.steps, 1)
+
+    def results():
+        out = []
+        for f in filters:
+            r = f.collect()
+            out.append((r.hit_offsets.copy(), r.line_start.copy(), r.line_end.copy(), ff_digest(f)))
+        return out
+
+    # every form starts from cleared feed-forward filters, so each form's results stand alone
+    for f in filters:
+        f.clear_ff()
+    t_plain, l_plain = timed(plain_serial)
+    ref = results()
+    for f in filters:
+        f.clear_ff()
+    t_streams, l_streams = timed(plain_streams)
+    got_streams = results()
+    for f in filters:
+        f.clear_ff()
+    t_batch, l_batch = timed(batched)
+    bst = torch.cuda.ExternalStream(b.stream, device=dev)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    dev_ms = []
+    for _ in range(args.steps):
+        e0.record(bst)
+        b.launch()
+        e1.record(bst)
+        b.wait()
+        dev_ms.append(e0.elapsed_time(e1))
+    got_batch = results()
+
+    def same(x, y):
+        return all(np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1]) and np.array_equal(a[2], c[2])
+                   and a[3] == c[3] for a, c in zip(x, y))
+
+    out = {
+        "workload": f"batched: {len(jobs)} jobs, {sum(w.n_patterns for w in jobs)} patterns (per job 1k-256k "
+                    f"log-uniform, 24-48 B, LEN 24), {nbytes / 2**30:.2f} GiB text (per job 256 KiB-"
+                    f"{args.batch_max_text >> 20} MiB log-uniform), 0.01% of windows planted",
+        "text_bytes": nbytes, "jobs": len(jobs), "hit_windows": sum(int(r[0].size) for r in ref),
+        "batched_gbs": nbytes / t_batch / 1e9,
+        "batched_device_gbs": nbytes / (statistics.median(dev_ms) * 1e-3) / 1e9,
+        "plain_serial_gbs": nbytes / t_plain / 1e9, "plain_streams_gbs": nbytes / t_streams / 1e9,
+        "batched_over_plain_serial": t_plain / t_batch, "batched_over_plain_streams": t_streams / t_batch,
+        "launches_per_step": {"batched": int(l_batch), "plain_serial": int(l_plain), "plain_streams": int(l_streams)},
+        "ms_per_step": {"batched": t_batch * 1e3, "batched_device": statistics.median(dev_ms),
+                        "plain_serial": t_plain * 1e3, "plain_streams": t_streams * 1e3},
+        "bit_exact": {"plain_streams_vs_plain": same(got_streams, ref), "batched_vs_plain": same(got_batch, ref)},
+        "setup_s": {"generate_and_build": gen_s, "batch_prepare": prepare_s},
+        "timing": "host clock between device-idle points, median of steps; batched_device = CUDA events",
+    }
+    b.close()
+    for f in filters:
+        f.close()
+    del d_all
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---- our arm --------------------------------------------------------------------------------------------
 def main_ours(args):
     import torch
@@ -292,6 +442,9 @@ def main_ours(args):
         t = torch.tensor([x], dtype=torch.float64, device=dev)
         dist.all_reduce(t, op=dist.ReduceOp.MAX)
         return float(t.item())
+
+    if args.workload == "batched":
+        return main_batched(args, world, rank, local, barrier, max_over_ranks)
 
     wl = workload(args)
     seed = args.seed + rank  # independent replicas
@@ -379,6 +532,40 @@ def main_ours(args):
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                                     "sample": f"failed: {e}"}
     f.close()
+    del d_text, host
+    torch.cuda.empty_cache()
+    if world == 1 and args.workload == "scale" and not args.no_batched:
+        # the batched form against plain per-job launches (its own workload, same GPU)
+        line["batched"] = run_batched(args, local)
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main_batched(args, world, rank, local, barrier, max_over_ranks):
+    """Headline line for the batched workload: value = device-timed GB/s of one batch launch."""
+    import torch.distributed as dist
+
+    sampler = ClockSampler(gpu_id_for(local))
+    sampler.start()
+    barrier()
+    r = run_batched(args, local)
+    clocks = sampler.stop()
+    ms = max_over_ranks(r["ms_per_step"]["batched_device"])
+    value = world * r["text_bytes"] / (ms * 1e-3) / 1e9
+    achieved = r["text_bytes"] / (ms * 1e-3) / 1e9
+    peak, peak_kind = measured_peaks()
+    line = {"metric": "batched vs plain GB/s", "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": r["workload"], "l2": "inputs larger than L2 (19 GiB of text), no flush",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                         "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
+                         "algorithmic_bytes_per_launch": r["text_bytes"]},
+            "gpu_launches": r["launches_per_step"]["batched"] * args.steps, "clocks": clocks, "batched": r}
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:

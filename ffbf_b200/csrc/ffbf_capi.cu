@@ -126,7 +126,9 @@ struct ffbf_batch {
     std::vector<Job> jobs;
     bool prepared = false;
     std::vector<void*> allocs;
-    uint32_t* d_error = nullptr;
+    uint32_t* d_error = nullptr;  // n_ctl groups of 4 words: error flags, work-queue counter
+    uint32_t n_ctl = 0;
+    uint64_t graph_kernels = 0;  // kernel nodes of the graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
     std::function<cudaError_t()> direct;  // the same launches without a graph (FFBF_BATCH_NOGRAPH=1)
@@ -1112,14 +1114,17 @@ ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
     TRY(balloc(b, &d_fast, fast.size() + 1));
     TRY(balloc(b, &d_args, args.size() + 1));
     TRY(balloc(b, &d_tail, tail.size() + 1));
+    // per tuned launch: 4 control words (error flags, work-queue counter), zeroed with the job counters
+    TRY(balloc(b, &b->d_error, 4 * (launches.size() + 1)));
+    b->n_ctl = (uint32_t)launches.size() + 1;
+    for (uint32_t i = 0; i < b->n_ctl; i++) counters.push_back(b->d_error + 4 * i);
     TRY(balloc(b, &d_counters, counters.size() + 1));
-    TRY(balloc(b, &b->d_error, 1));
     if ((fast.size() && cudaMemcpy(d_fast, fast.data(), fast.size() * sizeof(ffbf::FastJob), cudaMemcpyHostToDevice)) ||
         (args.size() && cudaMemcpy(d_args, args.data(), args.size() * sizeof(ffbf::ScanArgs), cudaMemcpyHostToDevice)) ||
         (tail.size() && cudaMemcpy(d_tail, tail.data(), tail.size() * sizeof(uint2), cudaMemcpyHostToDevice)) ||
         (counters.size() &&
          cudaMemcpy(d_counters, counters.data(), counters.size() * sizeof(uint32_t*), cudaMemcpyHostToDevice)) ||
-        cudaMemset(b->d_error, 0, sizeof(uint32_t)))
+        cudaMemset(b->d_error, 0, 16 * b->n_ctl))
         return bfail(b, FFBF_ECUDA, "batch table upload failed");
     const char* dbg = getenv("FFBF_BATCH_DEBUG");
     if (dbg && dbg[0] == '1') {
@@ -1133,12 +1138,13 @@ ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
             return FFBF_OK;
         };
         TRY(check(ffbf::zero_counters(d_counters, (uint32_t)counters.size(), b->st), "zero_counters"));
-        for (const Launch& L : launches) {
+        for (size_t li = 0; li < launches.size(); li++) {
+            const Launch& L = launches[li];
             char what[96];
             snprintf(what, sizeof what, "tuned launch len %u threads %d mode %d jobs %u items %u", L.len,
                      ffbf::config_threads(L.cfg), L.cfg.mode, L.n_jobs, L.n_items);
-            TRY(check(ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error,
-                                             b->num_sms, b->st),
+            TRY(check(ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1,
+                                             b->d_error + 4 * li, b->num_sms, b->st),
                       what));
         }
         TRY(check(ffbf::scan_generic_multi(d_args, d_tail, (uint32_t)tail.size(), b->num_sms, b->st), "generic tail"));
@@ -1147,10 +1153,10 @@ ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
         const uint32_t n_counters = (uint32_t)counters.size(), n_tail = (uint32_t)tail.size();
         b->direct = [=]() {
             cudaError_t e = ffbf::zero_counters(d_counters, n_counters, b->st);
-            for (const Launch& L : launches) {
-                if (e != cudaSuccess) break;
-                e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error,
-                                           b->num_sms, b->st);
+            for (size_t li = 0; li < launches.size() && e == cudaSuccess; li++) {
+                const Launch& L = launches[li];
+                e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1,
+                                           b->d_error + 4 * li, b->num_sms, b->st);
             }
             if (e == cudaSuccess) e = ffbf::scan_generic_multi(d_args, d_tail, n_tail, b->num_sms, b->st);
             return e;
@@ -1159,14 +1165,17 @@ ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
     // one graph: zero the jobs' counters, one tuned launch per group, one generic launch for all tail tiles
     if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return bfail(b, FFBF_ECUDA, "stream capture failed to start");
+    const uint64_t launches0 = ffbf::launches_total();
     cudaError_t e = ffbf::zero_counters(d_counters, (uint32_t)counters.size(), b->st);
-    for (const Launch& L : launches) {
-        if (e != cudaSuccess) break;
-        e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error, b->num_sms,
-                                   b->st);
+    for (size_t li = 0; li < launches.size() && e == cudaSuccess; li++) {
+        const Launch& L = launches[li];
+        e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error + 4 * li,
+                                   b->num_sms, b->st);
     }
     if (e == cudaSuccess) e = ffbf::scan_generic_multi(d_args, d_tail, (uint32_t)tail.size(), b->num_sms, b->st);
     cudaError_t e2 = cudaStreamEndCapture(b->st, &b->graph);
+    b->graph_kernels = ffbf::launches_total() - launches0;  // counted again at each graph launch
+    ffbf::unnote_launches(b->graph_kernels);
     if (e != cudaSuccess || e2 != cudaSuccess || cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
         cudaGetLastError();
         return bfail(b, FFBF_ECUDA, std::string("batch graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
@@ -1201,6 +1210,7 @@ ffbf_status ffbf_batch_launch(ffbf_batch* b) {
         cudaGetLastError();
         return bfail(b, FFBF_ECUDA, "graph launch failed");
     }
+    ffbf::note_launches(b->graph_kernels);
     return FFBF_OK;
 }
 
@@ -1213,8 +1223,12 @@ ffbf_status ffbf_batch_wait(ffbf_batch* b) {
         return bfail(b, FFBF_ECUDA, std::string("batch execution failed: ") + cudaGetErrorString(e));
     }
     uint32_t flag = 0;
-    if (b->d_error && cudaMemcpy(&flag, b->d_error, 4, cudaMemcpyDeviceToHost) != cudaSuccess)
-        return bfail(b, FFBF_ECUDA, "error flag read failed");
+    if (b->d_error) {
+        std::vector<uint32_t> ctl(4 * b->n_ctl);
+        if (cudaMemcpy(ctl.data(), b->d_error, 16 * b->n_ctl, cudaMemcpyDeviceToHost) != cudaSuccess)
+            return bfail(b, FFBF_ECUDA, "error flag read failed");
+        for (uint32_t i = 0; i < b->n_ctl; i++) flag |= ctl[4 * i];
+    }
     if (flag) {
         char buf[96];
         snprintf(buf, sizeof buf, "batched scan error flags 0x%x (4: a bounded wait gave up; others: self-checks)", flag);

@@ -11,6 +11,7 @@ namespace ffbf {
 
 static std::atomic<uint64_t> g_launches{0};
 void note_launches(uint64_t n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
+void unnote_launches(uint64_t n) { g_launches.fetch_sub(n, std::memory_order_relaxed); }
 uint64_t launches_total() { return g_launches.load(std::memory_order_relaxed); }
 
 // ------------------------------------------------------------------------------------------------

@@ -10,6 +10,8 @@ namespace ffbf {
 
 // Process-wide count of kernels launched by the library (reported through ffbf_kernel_launches).
 void note_launches(uint64_t n);
+// Takes back launches counted while a stream was being captured (they run when the graph does).
+void unnote_launches(uint64_t n);
 uint64_t launches_total();
 
 // One hit window: start offset in the text and its 64-bit rolling hash.
@@ -25,7 +27,9 @@ struct HitLine {
 };
 
 // Device counters shared by a scan: [0] hits found, [1] matches found, [2] error flags.
-enum { CNT_HITS = 0, CNT_MATCHES = 1, CNT_ERROR = 2, CNT_WORDS = 4 };
+// Per-scan counters: hit windows, verified matches, error flags, and the tuned scan's next-item counter
+// (its work queue); all four start at zero.
+enum { CNT_HITS = 0, CNT_MATCHES = 1, CNT_ERROR = 2, CNT_QUEUE = 3, CNT_WORDS = 4 };
 
 // Scan tile geometry of the generic kernel: each CTA stages TILE bytes (+ a 64-byte halo).
 constexpr int kScanThreads = 256;

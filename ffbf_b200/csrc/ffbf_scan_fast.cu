@@ -131,9 +131,15 @@ __device__ __forceinline__ bool full_check_from(const Geom& g, const uint32_t* _
 // probe `first` of all its entries before testing any, so its L2 round trips overlap; survivors finish the
 // test one by one.
 template <int PER_LANE>
-__device__ __noinline__ void flush_queue(const Geom g, const uint32_t* __restrict__ main_words, uint32_t* ff_words,
-                                         HitRec* hits, uint32_t hits_cap, uint32_t* counters, uint32_t qaddr, int qn,
-                                         uint64_t warp_row_pos0, uint64_t row_stride, int lane) {
+__device__ __noinline__ void flush_queue(const FastJob* J, uint32_t qaddr, int qn, uint64_t warp_row_pos0,
+                                         uint64_t row_stride, int lane) {
+    // the job's fields are read here rather than passed: the caller's loop keeps only its hot values live
+    const Geom g = J->g;
+    const uint32_t* __restrict__ main_words = J->main_words;
+    uint32_t* ff_words = J->ff_words;
+    HitRec* hits = J->hits;
+    const uint32_t hits_cap = J->hits_cap;
+    uint32_t* counters = J->counters;
     uint4 e[PER_LANE];
     uint32_t v[PER_LANE], bi[PER_LANE];
 #pragma unroll
@@ -186,7 +192,9 @@ __device__ __noinline__ void flush_queue(const Geom g, const uint32_t* __restric
 template <int L, int THREADS, int MODE>
 __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
                                                           uint32_t n_items, uint32_t max_s1_words,
-                                                          uint32_t* __restrict__ error_flag) {
+                                                          uint32_t* __restrict__ ctl) {
+    // ctl[0]: error flags; ctl[1]: the work queue, the count of items handed out past the first wave
+    uint32_t* const error_flag = ctl;
     constexpr int kStageBytes = THREADS * kRowBytes;
     constexpr int kQCap = MODE == 0 ? kQueueCap : 2 * kQueueCap;
     constexpr int kQBytes = kQCap * 16;
@@ -204,7 +212,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
     const uint32_t queues = bar0 + 128;
     const uint32_t s1 = queues + (THREADS / 32) * kQBytes;
     uint32_t* s1p = reinterpret_cast<uint32_t*>(smem + (s1 - base));
+    // Per-CTA state kept in shared memory rather than registers, which the dense mode's rings need:
+    // the load sequencer (thread 0 only), each warp's first text position of its current row, each
+    // thread's first and last '\n' so far in its stream.
     __shared__ int s_abort;
+    __shared__ uint32_t s_ni, s_nj;
+    __shared__ int s_nr;
+    __shared__ uint64_t s_wpos[THREADS / 32];
+    __shared__ long long s_fnl[THREADS], s_lnl[THREADS];
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     {
@@ -215,10 +230,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
         }
     }
     // load sequencer, run by thread 0: the next load is row nr (-1: halo) of item ni, which belongs to job nj
-    uint32_t ni = blockIdx.x, nj = 0;
-    int nr = -1;
     auto issue = [&](uint32_t k) {
         int* m = meta + 4 * (k & 1);
+        uint32_t ni = s_ni, nj = s_nj;
+        int nr = s_nr;
         if (ni >= n_items) {
             m[3] = 0;
             return;
@@ -240,11 +255,17 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             tma_load_3d(dst + b * kBox * kRowBytes, &J->tmap, 0, y, z + b * kBox, bar);
         if (++nr == (int)R) {
             nr = -1;
-            ni += gridDim.x;
+            ni = gridDim.x + atomicAdd(ctl + 1, 1u);  // next item from the queue
         }
+        s_ni = ni;
+        s_nj = nj;
+        s_nr = nr;
     };
     if (tid == 0) {
         s_abort = 0;
+        s_ni = blockIdx.x;
+        s_nj = 0;
+        s_nr = -1;
         mbar_init(bar0, 1);
         mbar_init(bar1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
@@ -258,22 +279,23 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
 
     // the current job's parameters (reloaded when the job changes)
     int cur_job = -1;
-    Geom g{};
     uint32_t R = 0, cmask = 0, s1_bmask = 0, p2_mask = 0, p2_add = 0, s1_first = 0, spt_log2 = 0;
     bool two = false;
-    uint64_t n_streams = 0;
-    const FastJob* J = jobs;
+    auto job_desc = [&]() { return jobs + cur_job; };
+    // The filter pointer is held in a register: the loop's global stores would otherwise make the compiler
+    // reload it from the descriptor before every probe. Fields used once per row or per queue flush are
+    // read from the descriptor where they are used, so they hold no registers across the byte loop.
+    const uint32_t* main_words = nullptr;
+    bool s1_fits = true;
 
     int qn = 0;  // warp-uniform queue fill
-    uint64_t warp_row_pos0 = 0, row_stride = 0;
     // Appends the lanes with `pass` to the warp queue; flushes when fewer than 32 slots remain.
     auto enqueue = [&](bool pass, uint32_t pos, uint32_t ql, uint32_t qh, uint32_t first) {
         const unsigned m = __ballot_sync(0xffffffffu, pass);
         if (m) {
             if (pass) {
+                // qn <= kQCap - 32 holds on entry (the queue flushes above that), so slot < kQCap
                 const uint32_t slot = (uint32_t)qn + __popc(m & lt_mask);
-                if (slot >= (uint32_t)kQCap) atomicOr(error_flag, 0x800u);
-                else
                 asm volatile("st.shared.v4.u32 [%0], {%1, %2, %3, %4};" ::"r"(qaddr + 16u * slot),
                              "r"(pos | ((uint32_t)lane << 8)), "r"(ql), "r"(qh), "r"(first)
                              : "memory");
@@ -281,8 +303,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             qn += __popc(m);
             if (qn > kQCap - 32) {
                 __syncwarp();
-                flush_queue<kQCap / 32>(g, J->main_words, J->ff_words, J->hits, J->hits_cap, J->counters, qaddr, qn,
-                                        warp_row_pos0, row_stride, lane);
+                flush_queue<kQCap / 32>(job_desc(), qaddr, qn, s_wpos[warp], (uint64_t)R * kRowBytes, lane);
                 qn = 0;
             }
         }
@@ -296,7 +317,6 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
 
     uint32_t hl = 0, hh = 0;
     int lnp = -1000;  // last '\n' relative to the current row start
-    long long first_nl = LLONG_MAX, last_nl = -1;
     uint32_t prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
 
     for (uint32_t k = 0;; k++) {
@@ -327,11 +347,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
         }
         if (job != cur_job) {
             cur_job = job;
-            J = jobs + job;
-            g = J->g;
+            const FastJob* J = job_desc();
+            const Geom g = J->g;
             R = J->rows;
-            n_streams = J->n_streams;
             spt_log2 = J->streams_per_tile_log2;
+            main_words = J->main_words;
+            s1_fits = MODE != 0 || J->stage1_nwords <= max_s1_words;
             cmask = g.cache_mask;
             two = g.s > 1;
             // stage-1 table of T = C >> shift bits, folded modulo T: the byte offset of bit (h & (T-1))'s
@@ -343,7 +364,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             // sparse mode: the stage-1 probes are exact when the table is the cache region itself
             s1_first = J->stage1_shift == 0 ? (two ? 2u : 1u) : 0u;
             if constexpr (MODE == 0) {
-                const uint32_t nw = J->stage1_nwords;
+                const uint32_t nw = s1_fits ? J->stage1_nwords : 0u;
                 const uint32_t* src = J->stage1_words;
                 for (uint32_t i = tid; i < nw; i += THREADS) s1p[i] = src[i];
                 __syncthreads();
@@ -351,14 +372,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
         }
 
         // self-checks: a bad descriptor or sequencing records a code and skips the work
-        if ((uint32_t)job >= n_jobs || st >= J->n_supertiles || r < -1 || r >= (int)R ||
-            (MODE == 0 && J->stage1_nwords > max_s1_words)) {
+        if ((uint32_t)job >= n_jobs || st >= job_desc()->n_supertiles || r < -1 || r >= (int)R || !s1_fits) {
             if (tid == 0) atomicOr(error_flag, 0x100u);
             __syncthreads();
             continue;
         }
         const uint64_t z = (uint64_t)st * THREADS + tid;
-        const bool active = z < n_streams;
+        const bool active = z < job_desc()->n_streams;
         const uint8_t* row = smem + (k & 1) * kStageBytes + tid * kRowBytes;
         const int sw = tid & 7;
 
@@ -391,13 +411,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                 if (c == 0x0Au) lnp = j - 32;
             }
             if (z == 0) lnp = -1;  // text start: nothing before offset 0
-            first_nl = LLONG_MAX;
-            last_nl = -1;
+            s_fnl[tid] = LLONG_MAX;
+            s_lnl[tid] = -1;
         } else {
             const int lnp_in = lnp;
             qn = 0;
-            warp_row_pos0 = ((uint64_t)st * THREADS + (uint64_t)warp * 32) * R * kRowBytes + (uint64_t)r * kRowBytes;
-            row_stride = (uint64_t)R * kRowBytes;
+            if (lane == 0)
+                s_wpos[warp] = ((uint64_t)st * THREADS + (uint64_t)warp * 32) * R * kRowBytes + (uint64_t)r * kRowBytes;
+            const bool need_first = s_fnl[tid] == LLONG_MAX;
             int row_first = -1;  // first '\n' of this row, found once per stream
 #pragma unroll 1
             for (int b = 0; b < kRowBytes / 32; b++) {
@@ -440,14 +461,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                         const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], ring_l[slot]) & 1u) != 0;
                         ring2_l[slot] = ring_l[slot];
                         ring2_h[slot] = ring_h[slot];
-                        ring2_v[slot] = ldg_if(J->main_words + (((ring_h[slot] & p2_mask) + p2_add) >> 5), pass1);
+                        ring2_v[slot] = ldg_if(main_words + (((ring_h[slot] & p2_mask) + p2_add) >> 5), pass1);
                         const bool valid = active && (j - lnp >= L);
                         ring_l[slot] = hl;
                         ring_h[slot] = hh;
-                        ring_v[slot] = ldg_if(J->main_words + ((hl & cmask) >> 5), valid);
+                        ring_v[slot] = ldg_if(main_words + ((hl & cmask) >> 5), valid);
                     }
                 }
-                if (lnp != lnp_blk && row_first < 0 && first_nl == LLONG_MAX) {
+                if (lnp != lnp_blk && row_first < 0 && need_first) {
                     for (int q = 0; q < 8 && row_first < 0; q++) {
                         const uint32_t t = cur[q] ^ 0x0A0A0A0Au;
                         const uint32_t zb = ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
@@ -473,19 +494,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             }
             if (qn) {
                 __syncwarp();
-                flush_queue<kQCap / 32>(g, J->main_words, J->ff_words, J->hits, J->hits_cap, J->counters, qaddr, qn,
-                                        warp_row_pos0, row_stride, lane);
+                flush_queue<kQCap / 32>(job_desc(), qaddr, qn, s_wpos[warp], (uint64_t)R * kRowBytes, lane);
                 qn = 0;
             }
             // lnp is now relative to the next row's start; lnp + 128 is its position in this row
             if (active && lnp + kRowBytes != lnp_in) {
                 const long long row_pos = (long long)(z * R + (uint32_t)r) * kRowBytes;
-                if (first_nl == LLONG_MAX) first_nl = row_pos + row_first;
-                last_nl = row_pos + lnp + kRowBytes;
+                if (need_first) s_fnl[tid] = row_pos + row_first;
+                s_lnl[tid] = row_pos + lnp + kRowBytes;
             }
             if ((uint32_t)r == R - 1) {
                 // per-16 KiB-tile newline summary: reduce over the lanes whose streams share the tile
-                long long f = active ? first_nl : LLONG_MAX, l = active ? last_nl : -1;
+                long long f = active ? s_fnl[tid] : LLONG_MAX, l = active ? s_lnl[tid] : -1;
                 const int G = 1 << spt_log2;
                 for (int o = 1; o < G; o <<= 1) {
                     f = min(f, __shfl_xor_sync(0xffffffffu, f, o));
@@ -493,6 +513,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                 }
                 if (active && (lane & (G - 1)) == 0) {
                     const uint64_t tile = z >> spt_log2;
+                    const FastJob* J = job_desc();
                     if (tile < J->n_tiles) {
                         J->tile_first_nl[tile] = f;
                         J->tile_last_nl[tile] = l;
@@ -518,6 +539,9 @@ PFN_cuTensorMapEncodeTiled_v12000 encoder() {
     return fn;
 }
 
+// static shared memory of k_scan_fast<., THREADS, .> (sequencer, row positions, per-thread newline state)
+constexpr size_t static_smem(int threads) { return 16 * (size_t)threads + 8 * (size_t)(threads / 32) + 64; }
+
 template <int THREADS, int MODE>
 constexpr size_t fixed_smem() {
     return 1024 + 2 * (size_t)THREADS * kRowBytes + kTabBytes + 128 +
@@ -526,26 +550,26 @@ constexpr size_t fixed_smem() {
 
 template <int L, int THREADS, int MODE>
 cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items, uint32_t max_s1_words,
-                       uint32_t* d_error, int num_sms, cudaStream_t st) {
+                       uint32_t* d_ctl, int num_sms, cudaStream_t st) {
     const size_t smem = fixed_smem<THREADS, MODE>() + (MODE == 0 ? 4 * (size_t)max_s1_words : 0);
     cudaError_t e =
         cudaFuncSetAttribute(k_scan_fast<L, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
     const int grid = (int)(n_items < (uint32_t)num_sms ? n_items : (uint32_t)num_sms);
     if (grid == 0) return cudaSuccess;
-    k_scan_fast<L, THREADS, MODE><<<grid, THREADS, smem, st>>>(d_jobs, n_jobs, n_items, max_s1_words, d_error);
+    k_scan_fast<L, THREADS, MODE><<<grid, THREADS, smem, st>>>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl);
     note_launches(1);
     return cudaGetLastError();
 }
 
 template <int L>
 cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
-                       uint32_t max_s1_words, uint32_t* d_error, int num_sms, cudaStream_t st) {
-    if (cfg.mode == 1) return launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_error, num_sms, st);
+                       uint32_t max_s1_words, uint32_t* d_ctl, int num_sms, cudaStream_t st) {
+    if (cfg.mode == 1) return launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
     switch (cfg.threads) {
-        case 256: return launch_cfg<L, 256, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
-        case 384: return launch_cfg<L, 384, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
-        default: return launch_cfg<L, 512, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        case 256: return launch_cfg<L, 256, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+        case 384: return launch_cfg<L, 384, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+        default: return launch_cfg<L, 512, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
     }
 }
 
@@ -577,7 +601,7 @@ bool fast_scan_supported(const Geom& g, uint64_t n) {
 
 // Largest power-of-two stage-1 table (in bits, <= C) that fits beside the fixed shared-memory layout.
 uint32_t stage1_shift_for(const Geom& g, int threads) {
-    const size_t room = kSmemLimit - fixed_smem_for(threads) - 64;
+    const size_t room = kSmemLimit - fixed_smem_for(threads) - static_smem(threads) - 64;
     uint32_t sh = 0;
     while (((uint64_t)g.cache_bits >> sh) / 8 > room) sh++;
     return sh;
@@ -643,14 +667,14 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
 }
 
 cudaError_t launch_fast_jobs(uint32_t len, const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs,
-                             uint32_t n_items, uint32_t max_s1_words, uint32_t* d_error, int num_sms,
+                             uint32_t n_items, uint32_t max_s1_words, uint32_t* d_ctl, int num_sms,
                              cudaStream_t st) {
     switch (len) {
-        case 16: return launch_len<16>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
-        case 19: return launch_len<19>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
-        case 20: return launch_len<20>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
-        case 24: return launch_len<24>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
-        case 32: return launch_len<32>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_error, num_sms, st);
+        case 16: return launch_len<16>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+        case 19: return launch_len<19>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+        case 20: return launch_len<20>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+        case 24: return launch_len<24>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+        case 32: return launch_len<32>(cfg, d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
         default: return cudaErrorInvalidValue;
     }
 }
@@ -678,7 +702,7 @@ cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, const Fas
         e = cudaMemcpyAsync(d_job, h_job, sizeof(FastJob), cudaMemcpyHostToDevice, st);
         if (e != cudaSuccess) return e;
         e = launch_fast_jobs(a.g.len, cfg, d_job, 1, h_job->n_supertiles, h_job->stage1_nwords,
-                             a.counters + CNT_ERROR, num_sms, st);
+                             a.counters + CNT_ERROR, num_sms, st);  // ctl = {CNT_ERROR, CNT_QUEUE}
         if (e != cudaSuccess) return e;
     }
     return scan_tail(a, covered, st);

@@ -62,8 +62,9 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
 cudaError_t scan_tail(const ScanArgs& a, uint64_t covered, cudaStream_t st);
 
 // One launch of the tuned kernel over n_jobs device-resident jobs sharing LEN and configuration.
+// d_ctl[0] collects error flags; d_ctl[1] is the work-queue counter and must be zero at launch.
 cudaError_t launch_fast_jobs(uint32_t len, const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs,
-                             uint32_t n_items, uint32_t max_s1_words, uint32_t* d_error, int num_sms, cudaStream_t st);
+                             uint32_t n_items, uint32_t max_s1_words, uint32_t* d_ctl, int num_sms, cudaStream_t st);
 
 // A plain scan: one job (h_job pinned host staging, d_job device copy) plus the generic tail.
 cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, const FastConfig& cfg, int num_sms,

@@ -9,6 +9,11 @@ Workloads (one uint64 seed each; patterns, then text, then planted occurrences):
               K 5, S 2, 2^23 cache bits (1 MiB), 2^26 external bits (8 MiB).
   binary      4,000,000 signatures of 16 uniform bytes ('\\n' redrawn), LEN 16; 8 GiB uniform text;
               100,000 planted. Geometry: the reference's defaults with LEN 16.
+  batched     512 independent jobs. Per job: a pattern count log-uniform in [1k, 256k] (printable, 24-48
+              bytes, LEN 24) and a text size log-uniform in [256 KiB, 256 MiB] (printable, '\\n' after
+              geometric(mean 80) bytes), with planted occurrences at 0.01% of the text's windows. Geometry
+              from a menu keyed on the pattern count: (2^20, 2^24) cache/external bits below 16k patterns,
+              (2^22, 2^26) below 64k, (2^23, 2^27) otherwise; K 5, S 2.
 Text sizes and plant counts scale together for the smaller parity cases (same densities).
 """
 import ctypes
@@ -120,3 +125,33 @@ def scale(text_bytes=4 * GiB, n_patterns=1_000_000):
 def binary(text_bytes=8 * GiB, n_patterns=4_000_000):
     return Workload("binary", Params(16, 5, 2, 1 << 24, 1 << 28), BINARY, n_patterns, 16, 16, 0, text_bytes,
                     max(1, round(100_000 * text_bytes / (8 * GiB))))
+
+
+def batch_geometry(n_patterns):
+    """The batched workload's geometry menu, keyed on the job's pattern count."""
+    if n_patterns < 16_000:
+        return Params(24, 5, 2, 1 << 20, 1 << 24)
+    if n_patterns < 64_000:
+        return Params(24, 5, 2, 1 << 22, 1 << 26)
+    return Params(24, 5, 2, 1 << 23, 1 << 27)
+
+
+def batched(n_jobs=512, pat_lo=1_000, pat_hi=256_000, text_lo=256 * 1024, text_hi=256 * MiB, seed=2024):
+    """The batched workload's jobs: one Workload per job, each with its own seed (Workload.seed).
+
+    Draws come from gen_u64 stream 3 of `seed`: per job one draw for its seed, one for the pattern count and
+    one for the text size, both log-uniform over [lo, hi] (floor(lo * (hi/lo)^u), u = draw / 2^64).
+    """
+    d = gen_u64(seed, 3, 3 * n_jobs).reshape(n_jobs, 3)
+    u_pat = d[:, 1].astype(np.float64) / 2.0**64
+    u_txt = d[:, 2].astype(np.float64) / 2.0**64
+    jobs = []
+    for j in range(n_jobs):
+        npat = int(pat_lo * (pat_hi / pat_lo) ** u_pat[j])
+        nbytes = int(text_lo * (text_hi / text_lo) ** u_txt[j])
+        n_windows = max(nbytes - 24 + 1, 0)
+        w = Workload(f"batched[{j}]", batch_geometry(npat), PRINTABLE, npat, 24, 48, 80, nbytes,
+                     max(1, round(1e-4 * n_windows)))
+        w.seed = int(d[j, 0])
+        jobs.append(w)
+    return jobs
