@@ -5,6 +5,6 @@ feed-forward bits, the feed-forward pattern prune and exact verification all run
 C ABI in include/ffbf.h. This package gives Python access to that ABI (lib.Filter) and to the seeded
 workload generator (datagen).
 """
-from .lib import DEFAULT_CHUNK, EXPORTED, Batch, FFBFError, Filter, Params, ScanOutput, format_spans, kernel_launches, load_library  # noqa: F401
+from .lib import DEFAULT_CHUNK, EXPORTED, Batch, FFBFError, Filter, Params, RequestResult, ScanOutput, Server, format_spans, kernel_launches, load_library  # noqa: F401
 
-__all__ = ["Batch", "DEFAULT_CHUNK", "EXPORTED", "FFBFError", "Filter", "Params", "ScanOutput", "format_spans", "kernel_launches", "load_library"]
+__all__ = ["Batch", "DEFAULT_CHUNK", "EXPORTED", "FFBFError", "Filter", "Params", "RequestResult", "ScanOutput", "Server", "format_spans", "kernel_launches", "load_library"]

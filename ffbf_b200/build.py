@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                   f"-I{os.path.join(ROOT, 'include')}"]
 
-CUDA_SOURCES = ["ffbf_kernels.cu", "ffbf_scan_fast.cu", "ffbf_capi.cu", "ffbf_static.cu"]
+CUDA_SOURCES = ["ffbf_kernels.cu", "ffbf_scan_fast.cu", "ffbf_capi.cu", "ffbf_batch.cu", "ffbf_serve.cu", "ffbf_static.cu"]
 
 
 def _newer(target, deps):
@@ -64,7 +64,7 @@ def build(force=False, verbose=False):
                 print(out)
     lib = os.path.join(OUT, "libffbf.so")
     if force or _newer(lib, objs):
-        _run([NVCC] + ARCH + ["-shared", "-cudart=static", "-o", lib + ".tmp"] + objs)
+        _run([NVCC] + ARCH + ["-shared", "-cudart=static", "-Xcompiler", "-pthread", "-o", lib + ".tmp"] + objs)
         os.replace(lib + ".tmp", lib)
     cli_src = os.path.join(CSRC, "ffbf_cli.cpp")
     cli = os.path.join(OUT, "ffbf")

@@ -20,121 +20,13 @@
 #include "ffbf_kernels.cuh"
 #include "ffbf_scan_fast.cuh"
 
+#include "ffbf_ctx.cuh"
+
 using ffbf::Geom;
 using ffbf::HitLine;
 using ffbf::HitRec;
 
-struct ffbf_ctx {
-    ffbf_params prm{};
-    Geom g{};
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t st = nullptr;
-    uint64_t budget = 0, used = 0;
-    std::map<void*, size_t> allocs;
-    std::string err;
-
-    uint32_t* d_main = nullptr;
-    uint32_t* d_ff = nullptr;
-    uint64_t filter_bytes = 0;
-    uint32_t* d_counters = nullptr;
-    uint32_t* h_counters = nullptr;  // pinned
-
-    // patterns
-    bool have_patterns = false;
-    std::vector<uint8_t> h_pat;
-    uint8_t* d_pat = nullptr;
-    uint64_t npat = 0;
-    uint64_t* d_pstart = nullptr;
-    uint64_t* d_pend = nullptr;
-    uint64_t* d_phash = nullptr;
-
-    // scan
-    uint8_t* d_text_own = nullptr;
-    size_t text_cap = 0;
-    const uint8_t* d_text = nullptr;
-    uint64_t text_len = 0;
-    bool scan_pending = false, have_scan = false;
-    HitRec* d_hits = nullptr;
-    HitLine* d_hitlines = nullptr;
-    uint32_t hits_cap = 0;
-    uint32_t nhits = 0;
-    long long* d_tiles = nullptr;  // 4 arrays of tiles_cap: first, last, prev, next
-    uint64_t tiles_cap = 0;
-    int scan_path = 0;             // 0 = generic, 1 = fast
-    uint32_t* d_stage1 = nullptr;  // stage-1 table of the tuned scan (cache copy or its fold)
-    bool stage1_dirty = true;
-    int stage1_threads = 0;        // CTA size the table was sized for
-    unsigned long long* d_popc = nullptr;
-    double stage1_fill = 0;
-    ffbf::FastConfig cfg{512, 0, 0};  // tuned-scan configuration (mode from the stage-1 fill, or the autotuner)
-    bool cfg_tuned = false;
-    int force_mode = -1;           // FFBF_SCAN_MODE=0|1 in the environment
-    bool force_generic = false;    // FFBF_FORCE_GENERIC_SCAN=1 in the environment
-    ffbf::FastJob* h_job = nullptr;  // pinned staging of a plain scan's job descriptor
-    ffbf::FastJob* d_job = nullptr;
-    std::vector<uint64_t> r_hits, r_ls, r_le;
-
-    // prune
-    bool have_prune = false;
-    uint64_t* d_ids = nullptr;
-    uint64_t nids = 0;
-    std::vector<uint64_t> r_ids;
-
-    // verify
-    uint64_t* d_keys = nullptr;
-    uint32_t* d_vals = nullptr;
-    uint64_t table_cap = 0;
-    uint64_t* d_moff = nullptr;
-    uint32_t* d_mpid = nullptr;
-    uint32_t match_cap = 0;
-    std::vector<uint64_t> r_moff, r_mpid;
-
-    // scratch for ordered compaction / codec
-    uint64_t* d_tmp = nullptr;
-    size_t tmp_words = 0;
-    uint8_t* d_small = nullptr;  // test_line input
-    size_t small_cap = 0;
-};
-
-struct ffbf_batch {
-    int device = 0;
-    int num_sms = 0;
-    cudaStream_t st = nullptr;
-    std::string err;
-    struct Job {
-        ffbf_ctx* c;
-        const uint8_t* text;
-        size_t len;
-    };
-    // The device buffers and configuration each job's descriptors were built from. A context that has
-    // since grown its hit buffer, reloaded its filter, added patterns or been retuned makes the batch
-    // prepare again before its next launch.
-    struct Key {
-        const void *main, *ff, *hits, *counters, *tiles, *stage1;
-        uint32_t hits_cap;
-        uint64_t tiles_cap;
-        int threads, mode;
-        uint32_t rows;
-        bool operator==(const Key& o) const {
-            return main == o.main && ff == o.ff && hits == o.hits && counters == o.counters && tiles == o.tiles &&
-                   stage1 == o.stage1 && hits_cap == o.hits_cap && tiles_cap == o.tiles_cap && threads == o.threads &&
-                   mode == o.mode && rows == o.rows;
-        }
-    };
-    std::vector<Key> keys;
-    std::vector<Job> jobs;
-    bool prepared = false;
-    std::vector<void*> allocs;
-    uint32_t* d_error = nullptr;  // n_ctl groups of 4 words: error flags, work-queue counter
-    uint32_t n_ctl = 0;
-    uint64_t graph_kernels = 0;  // kernel nodes of the graph
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t exec = nullptr;
-    std::function<cudaError_t()> direct;  // the same launches without a graph (FFBF_BATCH_NOGRAPH=1)
-};
-
-namespace {
+namespace ffbf_host {
 
 ffbf_status fail(ffbf_ctx* c, ffbf_status s, const char* fmt, ...) {
     if (c) {
@@ -148,21 +40,6 @@ ffbf_status fail(ffbf_ctx* c, ffbf_status s, const char* fmt, ...) {
     return s;
 }
 
-#define CUDA_TRY(c, expr)                                                                          \
-    do {                                                                                           \
-        cudaError_t e_ = (expr);                                                                   \
-        if (e_ != cudaSuccess) {                                                                   \
-            cudaGetLastError();                                                                    \
-            return fail((c), FFBF_ECUDA, "%s: %s (%s:%d)", #expr, cudaGetErrorString(e_), __FILE__, \
-                        __LINE__);                                                                 \
-        }                                                                                          \
-    } while (0)
-
-#define TRY(expr)                       \
-    do {                                \
-        ffbf_status s_ = (expr);        \
-        if (s_ != FFBF_OK) return s_;   \
-    } while (0)
 
 ffbf_status dalloc(ffbf_ctx* c, void** p, size_t bytes) {
     *p = nullptr;
@@ -179,26 +56,6 @@ ffbf_status dalloc(ffbf_ctx* c, void** p, size_t bytes) {
     c->used += bytes;
     c->allocs[*p] = bytes;
     return FFBF_OK;
-}
-
-template <class T>
-ffbf_status dalloc_t(ffbf_ctx* c, T** p, size_t count) {
-    void* v = nullptr;
-    ffbf_status s = dalloc(c, &v, count * sizeof(T));
-    *p = static_cast<T*>(v);
-    return s;
-}
-
-template <class T>
-void dfree(ffbf_ctx* c, T*& p) {
-    if (!p) return;
-    auto it = c->allocs.find((void*)p);
-    if (it != c->allocs.end()) {
-        c->used -= it->second;
-        c->allocs.erase(it);
-    }
-    cudaFree((void*)p);
-    p = nullptr;
 }
 
 ffbf_status ensure_tmp(ffbf_ctx* c, size_t words) {
@@ -292,7 +149,21 @@ const uint64_t kInitialHitsCap = 1u << 16;
 // unless the autotuner or the environment fixed it, the probe mode from the table's fill (the shared-memory
 // stage only pays while it rejects most windows).
 ffbf_status prepare_fast(ffbf_ctx* c) {
-    const int sparse_threads = c->cfg.mode == 1 && c->cfg_tuned ? ffbf::fast_scan_threads() : c->cfg.threads;
+    if (c->borrowed) {
+        // the filter's owner built the stage-1 table and chose the configuration
+        if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 1));
+        if (!c->h_job) {
+            if (cudaMallocHost(&c->h_job, sizeof(ffbf::FastJob)) != cudaSuccess) {
+                cudaGetLastError();
+                c->h_job = nullptr;
+                return fail(c, FFBF_ENOMEM_HOST, "pinned job descriptor");
+            }
+        }
+        if (!c->d_job) TRY(dalloc_t(c, &c->d_job, 1));
+        return FFBF_OK;
+    }
+    // the table is sized for the configured CTA (in the dense mode it only measures the filter's fill)
+    const int sparse_threads = c->cfg.threads;
     if (c->d_stage1 && c->stage1_threads != sparse_threads) {
         dfree(c, c->d_stage1);
         c->stage1_dirty = true;
@@ -326,11 +197,6 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
     return FFBF_OK;
 }
 
-ffbf_batch::Key batch_key(const ffbf_ctx* c) {
-    return ffbf_batch::Key{c->d_main, c->d_ff,          c->d_hits,      c->d_counters, c->d_tiles,
-                           c->d_stage1, c->hits_cap,    c->tiles_cap,   c->cfg.threads, c->cfg.mode,
-                           c->cfg.rows};
-}
 
 ffbf::ScanArgs make_scan_args(ffbf_ctx* c) {
     ffbf::ScanArgs a{};
@@ -392,7 +258,9 @@ ffbf_status setup_scan_state(ffbf_ctx* c, const uint8_t* d_text, size_t len) {
     return FFBF_OK;
 }
 
-}  // namespace
+}  // namespace ffbf_host
+
+using namespace ffbf_host;
 
 extern "C" {
 
@@ -472,8 +340,7 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
         return bail(FFBF_ECUDA);
     }
     const char* th = getenv("FFBF_SCAN_THREADS");
-    if (th) ffbf::set_fast_scan_threads(atoi(th));
-    c->cfg.threads = ffbf::fast_scan_threads();
+    if (th && (atoi(th) == 256 || atoi(th) == 384 || atoi(th) == 512)) c->cfg.threads = atoi(th);
     const char* fm = getenv("FFBF_SCAN_MODE");
     if (fm && (fm[0] == '0' || fm[0] == '1')) c->force_mode = fm[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");
@@ -481,6 +348,56 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
     *out = c;
     return FFBF_OK;
 }
+
+}  // extern "C"
+
+namespace ffbf_host {
+
+ffbf_status create_scan_slot(int device, ffbf_ctx** out) {
+    *out = nullptr;
+    ffbf_ctx* c = new (std::nothrow) ffbf_ctx();
+    if (!c) return FFBF_ENOMEM_HOST;
+    c->device = device;
+    c->borrowed = true;
+    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&c->st, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaDeviceGetAttribute(&c->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
+        cudaGetLastError();
+        ffbf_destroy(c);
+        return FFBF_ECUDA;
+    }
+    if (dalloc_t(c, &c->d_counters, ffbf::CNT_WORDS) != FFBF_OK) {
+        ffbf_destroy(c);
+        return FFBF_ENOMEM_DEVICE;
+    }
+    if (cudaMallocHost(&c->h_counters, ffbf::CNT_WORDS * sizeof(uint32_t)) != cudaSuccess) {
+        cudaGetLastError();
+        c->h_counters = nullptr;
+        ffbf_destroy(c);
+        return FFBF_ENOMEM_HOST;
+    }
+    *out = c;
+    return FFBF_OK;
+}
+
+void attach_filters(ffbf_ctx* slot, const ffbf_ctx* owner) {
+    slot->prm = owner->prm;
+    slot->g = owner->g;
+    slot->filter_bytes = owner->filter_bytes;
+    slot->d_main = owner->d_main;
+    slot->d_ff = owner->d_ff;
+    slot->d_stage1 = owner->d_stage1;
+    slot->stage1_threads = owner->stage1_threads;
+    slot->stage1_fill = owner->stage1_fill;
+    slot->stage1_dirty = false;
+    slot->cfg = owner->cfg;
+    slot->cfg_tuned = true;
+    slot->force_mode = owner->force_mode;
+    slot->force_generic = owner->force_generic;
+}
+
+}  // namespace ffbf_host
+
+extern "C" {
 
 void ffbf_destroy(ffbf_ctx* c) {
     if (!c) return;
@@ -963,334 +880,3 @@ ffbf_status ffbf_get_filters(ffbf_ctx* c, uint8_t* main_bits, uint8_t* ff_bits) 
 
 }  // extern "C"
 
-// ---- batched scans ---------------------------------------------------------------------------------------
-namespace {
-
-ffbf_status bfail(ffbf_batch* b, ffbf_status s, const std::string& msg) {
-    b->err = msg;
-    return s;
-}
-
-void batch_release(ffbf_batch* b) {
-    if (b->exec) cudaGraphExecDestroy(b->exec);
-    if (b->graph) cudaGraphDestroy(b->graph);
-    b->exec = nullptr;
-    b->graph = nullptr;
-    for (void* p : b->allocs) cudaFree(p);
-    b->allocs.clear();
-    b->d_error = nullptr;
-    b->prepared = false;
-    b->keys.clear();
-    cudaGetLastError();
-}
-
-template <class T>
-ffbf_status balloc(ffbf_batch* b, T** p, size_t count) {
-    void* v = nullptr;
-    if (cudaMalloc(&v, count * sizeof(T) + 16) != cudaSuccess) {
-        cudaGetLastError();
-        return bfail(b, FFBF_ENOMEM_DEVICE, "batch table allocation failed");
-    }
-    b->allocs.push_back(v);
-    *p = static_cast<T*>(v);
-    return FFBF_OK;
-}
-
-}  // namespace
-
-extern "C" {
-
-ffbf_status ffbf_batch_create(int device, ffbf_batch** out) {
-    if (!out) return FFBF_EINVAL;
-    *out = nullptr;
-    ffbf_batch* b = new (std::nothrow) ffbf_batch();
-    if (!b) return FFBF_ENOMEM_HOST;
-    b->device = device;
-    if (cudaSetDevice(device) != cudaSuccess || cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess ||
-        cudaDeviceGetAttribute(&b->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess) {
-        cudaGetLastError();
-        delete b;
-        return FFBF_ECUDA;
-    }
-    *out = b;
-    return FFBF_OK;
-}
-
-void ffbf_batch_destroy(ffbf_batch* b) {
-    if (!b) return;
-    cudaSetDevice(b->device);
-    if (b->st) cudaStreamSynchronize(b->st);
-    batch_release(b);
-    if (b->st) cudaStreamDestroy(b->st);
-    delete b;
-}
-
-const char* ffbf_batch_last_error(const ffbf_batch* b) { return b ? b->err.c_str() : "null batch"; }
-
-void* ffbf_batch_stream(ffbf_batch* b) { return b ? (void*)b->st : nullptr; }
-
-ffbf_status ffbf_batch_add(ffbf_batch* b, ffbf_ctx* c, const uint8_t* d_text, size_t len) {
-    if (!b || !c) return FFBF_EINVAL;
-    if (c->device != b->device) return bfail(b, FFBF_EINVAL, "context and batch are on different devices");
-    if (((uintptr_t)d_text & 15) != 0 || (!d_text && len)) return bfail(b, FFBF_EINVAL, "device text must be 16-byte aligned");
-    for (auto& j : b->jobs)
-        if (j.c == c) return bfail(b, FFBF_EINVAL, "a context may appear only once in a batch");
-    if (b->prepared) batch_release(b);
-    b->jobs.push_back({c, d_text, len});
-    return FFBF_OK;
-}
-
-ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
-    if (!b) return FFBF_EINVAL;
-    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, FFBF_ECUDA, "cudaSetDevice failed");
-    batch_release(b);
-    struct Group {
-        uint32_t len;
-        ffbf::FastConfig cfg;
-        std::vector<std::pair<uint64_t, ffbf::FastJob>> jobs;  // (bytes, descriptor)
-    };
-    std::vector<Group> groups;
-    std::vector<ffbf::ScanArgs> args;
-    std::vector<uint2> tail;
-    std::vector<uint32_t*> counters;
-    for (uint32_t i = 0; i < b->jobs.size(); i++) {
-        ffbf_ctx* c = b->jobs[i].c;
-        ffbf_status s = enter(c);
-        if (s == FFBF_OK) s = setup_scan_state(c, b->jobs[i].text, b->jobs[i].len);
-        if (s != FFBF_OK) return bfail(b, s, std::string("job setup: ") + c->err);
-        const ffbf::ScanArgs a = make_scan_args(c);
-        args.push_back(a);
-        counters.push_back(c->d_counters);
-        uint64_t covered = 0;
-        if (use_fast(c, a.n)) {
-            if ((s = prepare_fast(c)) != FFBF_OK) return bfail(b, s, std::string("job filter: ") + c->err);
-            const ffbf::FastConfig cfg = c->cfg;
-            const int threads = ffbf::config_threads(cfg);
-            const uint32_t rows = cfg.rows ? cfg.rows : ffbf::fast_rows(a.n, threads, b->num_sms, true);
-            ffbf::FastJob fj;
-            cudaError_t e;
-            covered = ffbf::fill_fast_job(a, c->d_stage1, cfg, rows, &fj, &e);
-            if (e != cudaSuccess) return bfail(b, FFBF_ECUDA, "tensor map encoding failed");
-            if (fj.n_supertiles) {
-                Group* gp = nullptr;
-                for (auto& g : groups)
-                    if (g.len == c->g.len && g.cfg.mode == cfg.mode && ffbf::config_threads(g.cfg) == threads) gp = &g;
-                if (!gp) {
-                    groups.push_back(Group{c->g.len, cfg, {}});
-                    gp = &groups.back();
-                }
-                gp->jobs.push_back({covered, fj});
-            }
-        }
-        for (uint64_t t = covered / ffbf::kScanTile; t < a.ntiles; t++) tail.push_back(make_uint2(i, (uint32_t)t));
-        if (cudaStreamSynchronize(c->st) != cudaSuccess) return bfail(b, FFBF_ECUDA, "context stream failed");
-        c->scan_pending = true;
-        b->keys.push_back(batch_key(c));
-    }
-    // descriptors: groups contiguous, largest jobs first within a group
-    std::vector<ffbf::FastJob> fast;
-    struct Launch {
-        uint32_t len;
-        ffbf::FastConfig cfg;
-        size_t off;
-        uint32_t n_jobs, n_items, max_s1;
-    };
-    std::vector<Launch> launches;
-    for (auto& g : groups) {
-        std::stable_sort(g.jobs.begin(), g.jobs.end(), [](const auto& x, const auto& y) { return x.first > y.first; });
-        Launch L{g.len, g.cfg, fast.size(), (uint32_t)g.jobs.size(), 0, 0};
-        for (auto& jb : g.jobs) {
-            jb.second.item_begin = L.n_items;
-            L.n_items += jb.second.n_supertiles;
-            L.max_s1 = std::max(L.max_s1, jb.second.stage1_nwords);
-            fast.push_back(jb.second);
-        }
-        launches.push_back(L);
-    }
-    ffbf::FastJob* d_fast = nullptr;
-    ffbf::ScanArgs* d_args = nullptr;
-    uint2* d_tail = nullptr;
-    uint32_t** d_counters = nullptr;
-    TRY(balloc(b, &d_fast, fast.size() + 1));
-    TRY(balloc(b, &d_args, args.size() + 1));
-    TRY(balloc(b, &d_tail, tail.size() + 1));
-    // per tuned launch: 4 control words (error flags, work-queue counter), zeroed with the job counters
-    TRY(balloc(b, &b->d_error, 4 * (launches.size() + 1)));
-    b->n_ctl = (uint32_t)launches.size() + 1;
-    for (uint32_t i = 0; i < b->n_ctl; i++) counters.push_back(b->d_error + 4 * i);
-    TRY(balloc(b, &d_counters, counters.size() + 1));
-    if ((fast.size() && cudaMemcpy(d_fast, fast.data(), fast.size() * sizeof(ffbf::FastJob), cudaMemcpyHostToDevice)) ||
-        (args.size() && cudaMemcpy(d_args, args.data(), args.size() * sizeof(ffbf::ScanArgs), cudaMemcpyHostToDevice)) ||
-        (tail.size() && cudaMemcpy(d_tail, tail.data(), tail.size() * sizeof(uint2), cudaMemcpyHostToDevice)) ||
-        (counters.size() &&
-         cudaMemcpy(d_counters, counters.data(), counters.size() * sizeof(uint32_t*), cudaMemcpyHostToDevice)) ||
-        cudaMemset(b->d_error, 0, 16 * b->n_ctl))
-        return bfail(b, FFBF_ECUDA, "batch table upload failed");
-    const char* dbg = getenv("FFBF_BATCH_DEBUG");
-    if (dbg && dbg[0] == '1') {
-        // diagnostic: the same launches, uncaptured, each checked before the next
-        auto check = [&](cudaError_t e, const char* what) -> ffbf_status {
-            if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
-            if (e != cudaSuccess) {
-                cudaGetLastError();
-                return bfail(b, FFBF_ECUDA, std::string(what) + ": " + cudaGetErrorString(e));
-            }
-            return FFBF_OK;
-        };
-        TRY(check(ffbf::zero_counters(d_counters, (uint32_t)counters.size(), b->st), "zero_counters"));
-        for (size_t li = 0; li < launches.size(); li++) {
-            const Launch& L = launches[li];
-            char what[96];
-            snprintf(what, sizeof what, "tuned launch len %u threads %d mode %d jobs %u items %u", L.len,
-                     ffbf::config_threads(L.cfg), L.cfg.mode, L.n_jobs, L.n_items);
-            TRY(check(ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1,
-                                             b->d_error + 4 * li, b->num_sms, b->st),
-                      what));
-        }
-        TRY(check(ffbf::scan_generic_multi(d_args, d_tail, (uint32_t)tail.size(), b->num_sms, b->st), "generic tail"));
-    }
-    {
-        const uint32_t n_counters = (uint32_t)counters.size(), n_tail = (uint32_t)tail.size();
-        b->direct = [=]() {
-            cudaError_t e = ffbf::zero_counters(d_counters, n_counters, b->st);
-            for (size_t li = 0; li < launches.size() && e == cudaSuccess; li++) {
-                const Launch& L = launches[li];
-                e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1,
-                                           b->d_error + 4 * li, b->num_sms, b->st);
-            }
-            if (e == cudaSuccess) e = ffbf::scan_generic_multi(d_args, d_tail, n_tail, b->num_sms, b->st);
-            return e;
-        };
-    }
-    // one graph: zero the jobs' counters, one tuned launch per group, one generic launch for all tail tiles
-    if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
-        return bfail(b, FFBF_ECUDA, "stream capture failed to start");
-    const uint64_t launches0 = ffbf::launches_total();
-    cudaError_t e = ffbf::zero_counters(d_counters, (uint32_t)counters.size(), b->st);
-    for (size_t li = 0; li < launches.size() && e == cudaSuccess; li++) {
-        const Launch& L = launches[li];
-        e = ffbf::launch_fast_jobs(L.len, L.cfg, d_fast + L.off, L.n_jobs, L.n_items, L.max_s1, b->d_error + 4 * li,
-                                   b->num_sms, b->st);
-    }
-    if (e == cudaSuccess) e = ffbf::scan_generic_multi(d_args, d_tail, (uint32_t)tail.size(), b->num_sms, b->st);
-    cudaError_t e2 = cudaStreamEndCapture(b->st, &b->graph);
-    b->graph_kernels = ffbf::launches_total() - launches0;  // counted again at each graph launch
-    ffbf::unnote_launches(b->graph_kernels);
-    if (e != cudaSuccess || e2 != cudaSuccess || cudaGraphInstantiate(&b->exec, b->graph, 0) != cudaSuccess) {
-        cudaGetLastError();
-        return bfail(b, FFBF_ECUDA, std::string("batch graph capture failed: ") + cudaGetErrorString(e != cudaSuccess ? e : e2));
-    }
-    b->prepared = true;
-    return FFBF_OK;
-}
-
-ffbf_status ffbf_batch_launch(ffbf_batch* b) {
-    if (!b) return FFBF_EINVAL;
-    bool stale = !b->prepared || b->keys.size() != b->jobs.size();
-    for (size_t i = 0; i < b->jobs.size() && !stale; i++)
-        stale = !(batch_key(b->jobs[i].c) == b->keys[i]) ||
-                (use_fast(b->jobs[i].c, b->jobs[i].len) && b->jobs[i].c->stage1_dirty);
-    if (stale) TRY(ffbf_batch_prepare(b));
-    if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, FFBF_ECUDA, "cudaSetDevice failed");
-    for (auto& j : b->jobs) {
-        reset_scan(j.c);
-        j.c->d_text = j.text;
-        j.c->text_len = j.len;
-        j.c->scan_pending = true;
-    }
-    const char* ng = getenv("FFBF_BATCH_NOGRAPH");
-    if (ng && ng[0] == '1') {
-        if (b->direct() != cudaSuccess) {
-            cudaGetLastError();
-            return bfail(b, FFBF_ECUDA, "direct batch launch failed");
-        }
-        return FFBF_OK;
-    }
-    if (cudaGraphLaunch(b->exec, b->st) != cudaSuccess) {
-        cudaGetLastError();
-        return bfail(b, FFBF_ECUDA, "graph launch failed");
-    }
-    ffbf::note_launches(b->graph_kernels);
-    return FFBF_OK;
-}
-
-ffbf_status ffbf_batch_wait(ffbf_batch* b) {
-    if (!b) return FFBF_EINVAL;
-    cudaError_t e = cudaSetDevice(b->device);
-    if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
-    if (e != cudaSuccess) {
-        cudaGetLastError();
-        return bfail(b, FFBF_ECUDA, std::string("batch execution failed: ") + cudaGetErrorString(e));
-    }
-    uint32_t flag = 0;
-    if (b->d_error) {
-        std::vector<uint32_t> ctl(4 * b->n_ctl);
-        if (cudaMemcpy(ctl.data(), b->d_error, 16 * b->n_ctl, cudaMemcpyDeviceToHost) != cudaSuccess)
-            return bfail(b, FFBF_ECUDA, "error flag read failed");
-        for (uint32_t i = 0; i < b->n_ctl; i++) flag |= ctl[4 * i];
-    }
-    if (flag) {
-        char buf[96];
-        snprintf(buf, sizeof buf, "batched scan error flags 0x%x (4: a bounded wait gave up; others: self-checks)", flag);
-        return bfail(b, (flag & 4u) ? FFBF_ETIMEOUT : FFBF_ECUDA, buf);
-    }
-    return FFBF_OK;
-}
-
-ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len, int* threads, int* mode) {
-    TRY(enter(c));
-    if (!d_text || ((uintptr_t)d_text & 15)) return fail(c, FFBF_EINVAL, "device text must be 16-byte aligned");
-    if (!use_fast(c, sample_len)) return fail(c, FFBF_EINVAL, "the tuned scan does not cover this geometry or size");
-    // keep the feed-forward filter: the trial scans set bits in it
-    uint32_t* saved = nullptr;
-    TRY(dalloc_t(c, &saved, c->filter_bytes / 4));
-    CUDA_TRY(c, cudaMemcpyAsync(saved, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
-    const ffbf::FastConfig cands[] = {{512, 0, 0}, {384, 0, 0}, {256, 0, 0}, {256, 1, 0}};
-    ffbf::FastConfig best = c->cfg;
-    float best_ms = 1e30f;
-    cudaEvent_t e0, e1;
-    cudaEventCreate(&e0);
-    cudaEventCreate(&e1);
-    const int saved_force = c->force_mode;
-    c->force_mode = -1;
-    ffbf_status s = FFBF_OK;
-    for (const auto& cand : cands) {
-        c->cfg = cand;
-        c->cfg_tuned = true;
-        ffbf::set_fast_scan_threads(cand.mode == 0 ? cand.threads : 0);
-        if ((s = setup_scan_state(c, d_text, sample_len)) != FFBF_OK) break;
-        float ms = 1e30f;
-        for (int rep = 0; rep < 3 && s == FFBF_OK; rep++) {
-            cudaEventRecord(e0, c->st);
-            s = launch_scan(c);
-            cudaEventRecord(e1, c->st);
-            if (cudaEventSynchronize(e1) != cudaSuccess) s = fail(c, FFBF_ECUDA, "autotune timing failed");
-            float t = 0;
-            cudaEventElapsedTime(&t, e0, e1);
-            if (rep > 0) ms = std::min(ms, t);  // the first run also builds the stage-1 table
-        }
-        if (s != FFBF_OK) break;
-        if (ms < best_ms) {
-            best_ms = ms;
-            best = cand;
-        }
-    }
-    c->force_mode = saved_force;
-    ffbf::set_fast_scan_threads(best.mode == 0 ? best.threads : 0);
-    c->cfg = best;
-    c->cfg_tuned = true;
-    reset_scan(c);
-    cudaEventDestroy(e0);
-    cudaEventDestroy(e1);
-    if (s == FFBF_OK) {
-        CUDA_TRY(c, cudaMemcpyAsync(c->d_ff, saved, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
-        s = sync(c);
-    }
-    dfree(c, saved);
-    if (s == FFBF_OK) s = prepare_fast(c);
-    if (threads) *threads = ffbf::config_threads(best);
-    if (mode) *mode = best.mode;
-    return s;
-}
-
-}  // extern "C"

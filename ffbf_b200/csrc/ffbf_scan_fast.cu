@@ -581,13 +581,7 @@ size_t fixed_smem_for(int threads) {
     }
 }
 
-int g_threads_override = 0;
-
 }  // namespace
-
-int fast_scan_threads() { return g_threads_override ? g_threads_override : 512; }
-
-void set_fast_scan_threads(int t) { g_threads_override = (t == 256 || t == 384 || t == 512) ? t : 0; }
 
 bool fast_scan_supported(const Geom& g, uint64_t n) {
     switch (g.len) {

@@ -41,9 +41,6 @@ struct FastConfig {
 // True when the tuned kernel handles this geometry and text size; otherwise the generic scan runs.
 bool fast_scan_supported(const Geom& g, uint64_t n);
 
-// Default CTA size of the sparse mode; anything other than 256/384/512 restores it.
-int fast_scan_threads();
-void set_fast_scan_threads(int threads);
 int config_threads(const FastConfig& cfg);
 
 // Stage-1 table of the sparse mode for a CTA size: a copy of the cache region when it fits in the shared

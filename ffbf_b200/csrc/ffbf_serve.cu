@@ -1,0 +1,532 @@
+// ffbf_serve.cu -- the scan server (ffbf_server_* in include/ffbf.h): resident pattern sets, admission of
+// requests by free slots and arena room, and continuous batching of the admitted requests.
+//
+// One host thread runs the loop. Per iteration it
+//   1. takes new submissions into the FIFO of pending requests;
+//   2. admits pending requests in order while a slot and a range of the text arena are free, and starts
+//      each one's host-to-device copy on the copy stream (an event marks its end);
+//   3. moves requests whose copy has finished to the ready list;
+//   4. when the previous launch sequence has finished, launches every ready request as one plan
+//      (build_plan/launch_plan: one tuned launch per (LEN, configuration) group, one generic launch for
+//      ragged ends) on the scan stream;
+//   5. collects one finished request: line resolution and the copy of its hits on the slot's own stream,
+//      which overlaps the next batch's scan; then frees its slot and arena range.
+// A slot is a context with its own scan buffers whose filters are attached from the request's set.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <chrono>
+#include <condition_variable>
+#include <cstdio>
+#include <deque>
+#include <map>
+#include <mutex>
+#include <new>
+#include <string>
+#include <thread>
+#include <unordered_map>
+#include <vector>
+
+#include "ffbf_ctx.cuh"
+
+using namespace ffbf_host;
+
+namespace {
+
+using Clock = std::chrono::steady_clock;
+
+struct Request {
+    uint64_t id = 0;
+    uint32_t set = 0;
+    const uint8_t* h_text = nullptr;
+    size_t len = 0;
+    uint64_t off = 0;
+    uint64_t span = 0;  // arena bytes held
+    int slot = -1;
+    double t_submit = 0, t_admit = 0, t_launch = 0, t_done = 0;
+    ffbf_status status = FFBF_OK;
+    std::vector<uint64_t> hits, ls, le;
+};
+
+constexpr uint64_t kArenaAlign = 256;
+constexpr uint32_t kMaxCtl = 64;  // control-word groups per plan (one per tuned launch, plus one)
+
+}  // namespace
+
+struct ffbf_server {
+    int device = 0;
+    int num_sms = 0;
+    cudaStream_t st_scan = nullptr, st_copy = nullptr;
+    Clock::time_point t0;
+    std::string err;
+
+    std::vector<ffbf_ctx*> sets;
+    std::vector<ffbf_ctx*> slots;
+    std::vector<cudaEvent_t> copy_done;  // per slot
+    std::vector<int> free_slots;
+
+    uint8_t* d_arena = nullptr;
+    uint64_t arena_bytes = 0;
+    std::map<uint64_t, uint64_t> free_ranges;  // offset -> length, coalesced
+
+    // plan tables on the device and their pinned staging
+    ffbf::FastJob* d_fast = nullptr;
+    ffbf::ScanArgs* d_args = nullptr;
+    uint32_t** d_counters = nullptr;
+    uint32_t* d_ctl = nullptr;
+    uint2* d_tail = nullptr;
+    size_t tail_cap = 0;
+    ffbf::FastJob* h_fast = nullptr;
+    ffbf::ScanArgs* h_args = nullptr;
+    uint32_t** h_counters = nullptr;
+    uint2* h_tail = nullptr;
+    uint32_t* h_ctl = nullptr;  // error flags read back after each batch
+    cudaEvent_t batch_done = nullptr;
+    uint32_t batch_ctl = 0;
+
+    std::thread worker;
+    std::mutex mu;
+    std::condition_variable cv_work, cv_done;
+    bool stop = false;
+    bool started = false;
+    std::deque<Request*> inbox;                    // guarded by mu
+    std::deque<Request*> done;                     // guarded by mu
+    std::unordered_map<uint64_t, Request*> owned;  // polled, not yet released (guarded by mu)
+    uint64_t next_id = 1;
+    ffbf_server_stats stats{};  // guarded by mu
+    ffbf_status fatal = FFBF_OK;
+
+    // worker-only state
+    std::deque<Request*> pending;
+    std::vector<Request*> copying, ready, running, collect;
+    bool in_flight = false;
+
+    double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
+};
+
+namespace {
+
+ffbf_status sfail(ffbf_server* s, ffbf_status st, const std::string& msg) {
+    s->err = msg;
+    return st;
+}
+
+bool arena_alloc(ffbf_server* s, uint64_t bytes, uint64_t* off) {
+    for (auto it = s->free_ranges.begin(); it != s->free_ranges.end(); ++it) {
+        if (it->second >= bytes) {
+            *off = it->first;
+            const uint64_t rest = it->second - bytes;
+            const uint64_t at = it->first + bytes;
+            s->free_ranges.erase(it);
+            if (rest) s->free_ranges[at] = rest;
+            return true;
+        }
+    }
+    return false;
+}
+
+void arena_free(ffbf_server* s, uint64_t off, uint64_t bytes) {
+    auto it = s->free_ranges.emplace(off, bytes).first;
+    auto next = std::next(it);
+    if (next != s->free_ranges.end() && it->first + it->second == next->first) {
+        it->second += next->second;
+        s->free_ranges.erase(next);
+    }
+    if (it != s->free_ranges.begin()) {
+        auto prev = std::prev(it);
+        if (prev->first + prev->second == it->first) {
+            prev->second += it->second;
+            s->free_ranges.erase(it);
+        }
+    }
+}
+
+// Ends a request: its slot and arena range return to the pools and it joins the finished queue.
+void finish(ffbf_server* s, Request* r, ffbf_status st) {
+    r->status = st;
+    r->t_done = s->now();
+    if (r->slot >= 0) s->free_slots.push_back(r->slot);
+    if (r->span) arena_free(s, r->off, r->span);
+    r->slot = -1;
+    r->span = 0;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stats.requests_done++;
+    if (st == FFBF_OK) s->stats.bytes_scanned += r->len;
+    s->done.push_back(r);
+    s->cv_done.notify_all();
+}
+
+void admit(ffbf_server* s) {
+    while (!s->pending.empty() && !s->free_slots.empty()) {
+        Request* r = s->pending.front();
+        const uint64_t span = (r->len + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
+        uint64_t off = 0;
+        if (span && !arena_alloc(s, span, &off)) break;  // in order: wait for room
+        s->pending.pop_front();
+        r->slot = s->free_slots.back();
+        s->free_slots.pop_back();
+        r->off = off;
+        r->span = span;
+        r->t_admit = s->now();
+        if (r->len && cudaMemcpyAsync(s->d_arena + off, r->h_text, r->len, cudaMemcpyHostToDevice, s->st_copy) !=
+                          cudaSuccess) {
+            cudaGetLastError();
+            finish(s, r, FFBF_ECUDA);
+            continue;
+        }
+        cudaEventRecord(s->copy_done[r->slot], s->st_copy);
+        s->copying.push_back(r);
+    }
+}
+
+bool ensure_tail(ffbf_server* s, size_t n) {
+    if (n <= s->tail_cap) return true;
+    size_t cap = std::max(n, 2 * s->tail_cap);
+    if (s->d_tail) cudaFree(s->d_tail);
+    if (s->h_tail) cudaFreeHost(s->h_tail);
+    s->d_tail = nullptr;
+    s->h_tail = nullptr;
+    s->tail_cap = 0;
+    if (cudaMalloc(&s->d_tail, cap * sizeof(uint2)) != cudaSuccess ||
+        cudaMallocHost(&s->h_tail, cap * sizeof(uint2)) != cudaSuccess) {
+        cudaGetLastError();
+        return false;
+    }
+    s->tail_cap = cap;
+    return true;
+}
+
+// Launches every ready request as one plan on the scan stream.
+void launch_ready(ffbf_server* s) {
+    std::vector<PlanJob> jobs;
+    std::vector<Request*> batch;
+    for (Request* r : s->ready) {
+        ffbf_ctx* slot = s->slots[r->slot];
+        attach_filters(slot, s->sets[r->set]);
+        jobs.push_back({slot, s->d_arena + r->off, r->len});
+        batch.push_back(r);
+    }
+    s->ready.clear();
+    ScanPlan plan;
+    size_t bad = 0;
+    ffbf_status st = build_plan(jobs, s->num_sms, plan, &bad);
+    if (st == FFBF_OK && plan.launches.size() + 1 > kMaxCtl) st = FFBF_EINVAL;
+    if (st == FFBF_OK && !ensure_tail(s, plan.tail.size() + 1)) st = FFBF_ENOMEM_DEVICE;
+    if (st != FFBF_OK) {
+        if (st != FFBF_EINVAL && bad < jobs.size()) s->err = jobs[bad].c->err;
+        for (Request* r : batch) finish(s, r, st);
+        return;
+    }
+    const uint32_t n = (uint32_t)jobs.size();
+    const uint32_t n_ctl = (uint32_t)plan.launches.size() + 1;
+    std::copy(plan.fast.begin(), plan.fast.end(), s->h_fast);
+    std::copy(plan.args.begin(), plan.args.end(), s->h_args);
+    std::copy(plan.tail.begin(), plan.tail.end(), s->h_tail);
+    for (uint32_t i = 0; i < n; i++) s->h_counters[i] = jobs[i].c->d_counters;
+    for (uint32_t i = 0; i < n_ctl; i++) s->h_counters[n + i] = s->d_ctl + 4 * i;
+    PlanDevice d{s->d_fast, s->d_args, s->d_tail, s->d_counters, n + n_ctl, s->d_ctl};
+    cudaError_t e = cudaSuccess;
+    auto up = [&](void* dst, const void* src, size_t bytes) {
+        if (e == cudaSuccess && bytes) e = cudaMemcpyAsync(dst, src, bytes, cudaMemcpyHostToDevice, s->st_scan);
+    };
+    up(s->d_fast, s->h_fast, plan.fast.size() * sizeof(ffbf::FastJob));
+    up(s->d_args, s->h_args, plan.args.size() * sizeof(ffbf::ScanArgs));
+    up(s->d_tail, s->h_tail, plan.tail.size() * sizeof(uint2));
+    up(s->d_counters, s->h_counters, (n + n_ctl) * sizeof(uint32_t*));
+    const double t = s->now();
+    if (e == cudaSuccess) e = launch_plan(plan, d, s->num_sms, s->st_scan);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->h_ctl, s->d_ctl, 16 * n_ctl, cudaMemcpyDeviceToHost, s->st_scan);
+    if (e == cudaSuccess) e = cudaEventRecord(s->batch_done, s->st_scan);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        s->err = std::string("batch launch failed: ") + cudaGetErrorString(e);
+        for (Request* r : batch) finish(s, r, FFBF_ECUDA);
+        return;
+    }
+    for (Request* r : batch) r->t_launch = t;
+    s->running = batch;
+    s->batch_ctl = n_ctl;
+    s->in_flight = true;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stats.batches++;
+    s->stats.max_batch = std::max<uint64_t>(s->stats.max_batch, n);
+}
+
+void collect_one(ffbf_server* s) {
+    Request* r = s->collect.front();
+    s->collect.erase(s->collect.begin());
+    ffbf_ctx* slot = s->slots[r->slot];
+    ffbf_scan_result res{};
+    ffbf_status st = ffbf_scan_collect(slot, &res);
+    if (st == FFBF_OK) {
+        r->hits.assign(res.hit_offsets, res.hit_offsets + res.n_hits);
+        r->ls.assign(res.line_start, res.line_start + res.n_lines);
+        r->le.assign(res.line_end, res.line_end + res.n_lines);
+    } else {
+        s->err = slot->err;
+    }
+    finish(s, r, st);
+}
+
+void worker_loop(ffbf_server* s) {
+    cudaSetDevice(s->device);
+    for (;;) {
+        {
+            std::unique_lock<std::mutex> lk(s->mu);
+            const bool idle = s->pending.empty() && s->copying.empty() && s->ready.empty() && !s->in_flight &&
+                              s->collect.empty();
+            if (idle && s->inbox.empty() && !s->stop) s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
+            while (!s->inbox.empty()) {
+                s->pending.push_back(s->inbox.front());
+                s->inbox.pop_front();
+            }
+            if (s->stop) break;
+        }
+        bool progress = false;
+        const size_t before = s->copying.size();
+        admit(s);
+        progress |= s->copying.size() != before;
+        for (size_t i = 0; i < s->copying.size();) {
+            Request* r = s->copying[i];
+            cudaError_t q = cudaEventQuery(s->copy_done[r->slot]);
+            if (q == cudaErrorNotReady) {
+                i++;
+                continue;
+            }
+            s->copying.erase(s->copying.begin() + i);
+            if (q != cudaSuccess) {
+                cudaGetLastError();
+                finish(s, r, FFBF_ECUDA);
+            } else {
+                s->ready.push_back(r);
+            }
+            progress = true;
+        }
+        if (s->in_flight) {
+            cudaError_t q = cudaEventQuery(s->batch_done);
+            if (q != cudaErrorNotReady) {
+                s->in_flight = false;
+                uint32_t flags = 0;
+                for (uint32_t i = 0; i < s->batch_ctl; i++) flags |= s->h_ctl[4 * i];
+                const ffbf_status st = q != cudaSuccess ? FFBF_ECUDA : flags & 4u ? FFBF_ETIMEOUT : flags ? FFBF_ECUDA : FFBF_OK;
+                if (q != cudaSuccess) cudaGetLastError();
+                for (Request* r : s->running) {
+                    if (st == FFBF_OK) s->collect.push_back(r);
+                    else finish(s, r, st);
+                }
+                s->running.clear();
+                progress = true;
+            }
+        }
+        if (!s->in_flight && !s->ready.empty()) {
+            launch_ready(s);
+            progress = true;
+        }
+        if (!s->collect.empty()) {
+            collect_one(s);
+            progress = true;
+        }
+        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(10));
+    }
+    // stopping: let the device finish what was issued, then drop what is left
+    cudaStreamSynchronize(s->st_copy);
+    cudaStreamSynchronize(s->st_scan);
+    for (auto* c : s->slots) cudaStreamSynchronize(c->st);
+    cudaGetLastError();
+}
+
+void server_free(ffbf_server* s) {
+    cudaSetDevice(s->device);
+    for (auto* c : s->slots) ffbf_destroy(c);
+    for (auto ev : s->copy_done) cudaEventDestroy(ev);
+    if (s->batch_done) cudaEventDestroy(s->batch_done);
+    for (void* p : {(void*)s->d_arena, (void*)s->d_fast, (void*)s->d_args, (void*)s->d_counters, (void*)s->d_ctl,
+                    (void*)s->d_tail})
+        if (p) cudaFree(p);
+    for (void* p : {(void*)s->h_fast, (void*)s->h_args, (void*)s->h_counters, (void*)s->h_tail, (void*)s->h_ctl})
+        if (p) cudaFreeHost(p);
+    if (s->st_scan) cudaStreamDestroy(s->st_scan);
+    if (s->st_copy) cudaStreamDestroy(s->st_copy);
+    auto drop = [](std::deque<Request*>& q) {
+        for (auto* r : q) delete r;
+        q.clear();
+    };
+    drop(s->inbox);
+    drop(s->pending);
+    drop(s->done);
+    for (auto* v : {&s->copying, &s->ready, &s->running, &s->collect}) {
+        for (auto* r : *v) delete r;
+        v->clear();
+    }
+    for (auto& kv : s->owned) delete kv.second;
+    s->owned.clear();
+    cudaGetLastError();
+    delete s;
+}
+
+}  // namespace
+
+extern "C" {
+
+ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots, ffbf_server** out) {
+    if (!out) return FFBF_EINVAL;
+    *out = nullptr;
+    ffbf_server* s = new (std::nothrow) ffbf_server();
+    if (!s) return FFBF_ENOMEM_HOST;
+    s->device = device;
+    s->t0 = Clock::now();
+    if (slots == 0) slots = 64;
+    auto bail = [&](ffbf_status st) {
+        server_free(s);
+        return st;
+    };
+    size_t free_b = 0, total_b = 0;
+    if (cudaSetDevice(device) != cudaSuccess || cudaMemGetInfo(&free_b, &total_b) != cudaSuccess ||
+        cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->st_scan, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->st_copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaEventCreateWithFlags(&s->batch_done, cudaEventDisableTiming) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(FFBF_ECUDA);
+    }
+    if (arena_bytes == 0) arena_bytes = free_b / 2;
+    arena_bytes = arena_bytes / kArenaAlign * kArenaAlign;
+    if (arena_bytes == 0 || arena_bytes > free_b) return bail(FFBF_ENOMEM_DEVICE);
+    if (cudaMalloc(&s->d_arena, arena_bytes) != cudaSuccess) {
+        cudaGetLastError();
+        return bail(FFBF_ENOMEM_DEVICE);
+    }
+    s->arena_bytes = arena_bytes;
+    s->free_ranges[0] = arena_bytes;
+    const size_t n_counters = slots + kMaxCtl;
+    if (cudaMalloc(&s->d_fast, slots * sizeof(ffbf::FastJob)) != cudaSuccess ||
+        cudaMalloc(&s->d_args, slots * sizeof(ffbf::ScanArgs)) != cudaSuccess ||
+        cudaMalloc(&s->d_counters, n_counters * sizeof(uint32_t*)) != cudaSuccess ||
+        cudaMalloc(&s->d_ctl, 16 * kMaxCtl) != cudaSuccess ||
+        cudaMallocHost(&s->h_fast, slots * sizeof(ffbf::FastJob)) != cudaSuccess ||
+        cudaMallocHost(&s->h_args, slots * sizeof(ffbf::ScanArgs)) != cudaSuccess ||
+        cudaMallocHost(&s->h_counters, n_counters * sizeof(uint32_t*)) != cudaSuccess ||
+        cudaMallocHost(&s->h_ctl, 16 * kMaxCtl) != cudaSuccess || !ensure_tail(s, 4096)) {
+        cudaGetLastError();
+        return bail(FFBF_ENOMEM_DEVICE);
+    }
+    for (uint32_t i = 0; i < slots; i++) {
+        ffbf_ctx* c = nullptr;
+        ffbf_status st = create_scan_slot(device, &c);
+        if (st != FFBF_OK) return bail(st);
+        s->slots.push_back(c);
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(FFBF_ECUDA);
+        }
+        s->copy_done.push_back(ev);
+        s->free_slots.push_back((int)(slots - 1 - i));
+    }
+    s->stats.arena_bytes = arena_bytes;
+    s->stats.slots = slots;
+    s->worker = std::thread(worker_loop, s);
+    *out = s;
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_server_add_set(ffbf_server* s, ffbf_ctx* set, uint32_t* set_id) {
+    if (!s || !set || !set_id) return FFBF_EINVAL;
+    if (set->device != s->device) return sfail(s, FFBF_EINVAL, "the set's context is on another device");
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        if (s->started) return sfail(s, FFBF_ESTATE, "sets are registered before the first submit");
+    }
+    ffbf_status st = enter(set);
+    if (st == FFBF_OK && ffbf::fast_scan_supported(set->g, ffbf::kScanTile) && !set->force_generic) st = prepare_fast(set);
+    if (st == FFBF_OK) st = sync(set);
+    if (st != FFBF_OK) return sfail(s, st, std::string("set preparation failed: ") + set->err);
+    *set_id = (uint32_t)s->sets.size();
+    s->sets.push_back(set);
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_server_submit(ffbf_server* s, uint32_t set_id, const uint8_t* text, size_t len, uint64_t* request_id) {
+    if (!s || !request_id) return FFBF_EINVAL;
+    if (set_id >= s->sets.size()) return sfail(s, FFBF_EINVAL, "unknown set");
+    if (!text && len) return sfail(s, FFBF_EINVAL, "text is NULL");
+    if ((len + kArenaAlign - 1) / kArenaAlign * kArenaAlign > s->arena_bytes)
+        return sfail(s, FFBF_EINVAL, "request text is larger than the server's text arena");
+    Request* r = new (std::nothrow) Request();
+    if (!r) return FFBF_ENOMEM_HOST;
+    r->set = set_id;
+    r->h_text = text;
+    r->len = len;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->started = true;
+        r->id = s->next_id++;
+        r->t_submit = s->now();
+        s->inbox.push_back(r);
+    }
+    s->cv_work.notify_one();
+    *request_id = r->id;
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_server_poll(ffbf_server* s, ffbf_request_result* out, uint32_t max, uint32_t* n_out,
+                             uint32_t wait_us) {
+    if (!s || !n_out || (max && !out)) return FFBF_EINVAL;
+    *n_out = 0;
+    std::unique_lock<std::mutex> lk(s->mu);
+    if (s->done.empty() && wait_us)
+        s->cv_done.wait_for(lk, std::chrono::microseconds(wait_us), [&] { return !s->done.empty(); });
+    while (*n_out < max && !s->done.empty()) {
+        Request* r = s->done.front();
+        s->done.pop_front();
+        s->owned[r->id] = r;
+        ffbf_request_result& o = out[(*n_out)++];
+        o.request_id = r->id;
+        o.set_id = r->set;
+        o.status = r->status;
+        o.text_len = r->len;
+        o.n_hits = r->hits.size();
+        o.hit_offsets = r->hits.data();
+        o.n_lines = r->ls.size();
+        o.line_start = r->ls.data();
+        o.line_end = r->le.data();
+        o.t_submit = r->t_submit;
+        o.t_admit = r->t_admit;
+        o.t_launch = r->t_launch;
+        o.t_done = r->t_done;
+    }
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_server_release(ffbf_server* s, uint64_t request_id) {
+    if (!s) return FFBF_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    auto it = s->owned.find(request_id);
+    if (it == s->owned.end()) return FFBF_EINVAL;
+    delete it->second;
+    s->owned.erase(it);
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_server_get_stats(ffbf_server* s, ffbf_server_stats* out) {
+    if (!s || !out) return FFBF_EINVAL;
+    std::lock_guard<std::mutex> lk(s->mu);
+    *out = s->stats;
+    return FFBF_OK;
+}
+
+const char* ffbf_server_last_error(const ffbf_server* s) { return s ? s->err.c_str() : "null server"; }
+
+void ffbf_server_destroy(ffbf_server* s) {
+    if (!s) return;
+    {
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stop = true;
+    }
+    s->cv_work.notify_all();
+    if (s->worker.joinable()) s->worker.join();
+    server_free(s);
+}
+
+}  // extern "C"

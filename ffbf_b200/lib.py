@@ -37,7 +37,9 @@ EXPORTED = [
     "ffbf_test_line", "ffbf_clear_ff", "ffbf_get_filters", "ffbf_filter_bytes", "ffbf_free", "ffbf_format_spans",
     "ffbf_stream", "ffbf_kernel_launches", "ffbf_scan_static", "ffbf_batch_create", "ffbf_batch_add",
     "ffbf_batch_prepare", "ffbf_batch_launch", "ffbf_batch_wait", "ffbf_batch_stream", "ffbf_batch_last_error",
-    "ffbf_batch_destroy", "ffbf_autotune",
+    "ffbf_batch_destroy", "ffbf_autotune", "ffbf_server_create", "ffbf_server_add_set", "ffbf_server_submit",
+    "ffbf_server_poll", "ffbf_server_release", "ffbf_server_get_stats", "ffbf_server_last_error",
+    "ffbf_server_destroy",
 ]
 
 
@@ -65,6 +67,20 @@ class Params(ctypes.Structure):
 
     def __repr__(self):
         return f"Params(len={self.len}, k={self.k}, s={self.s}, cache_bits={self.cache_bits:#x}, ext_bits={self.ext_bits:#x})"
+
+
+class _RequestResult(ctypes.Structure):
+    _fields_ = [("request_id", ctypes.c_uint64), ("set_id", ctypes.c_uint32), ("status", ctypes.c_int),
+                ("text_len", ctypes.c_uint64), ("n_hits", ctypes.c_uint64),
+                ("hit_offsets", ctypes.POINTER(ctypes.c_uint64)), ("n_lines", ctypes.c_uint64),
+                ("line_start", ctypes.POINTER(ctypes.c_uint64)), ("line_end", ctypes.POINTER(ctypes.c_uint64)),
+                ("t_submit", ctypes.c_double), ("t_admit", ctypes.c_double), ("t_launch", ctypes.c_double),
+                ("t_done", ctypes.c_double)]
+
+
+class _ServerStats(ctypes.Structure):
+    _fields_ = [("requests_done", ctypes.c_uint64), ("batches", ctypes.c_uint64), ("bytes_scanned", ctypes.c_uint64),
+                ("max_batch", ctypes.c_uint64), ("arena_bytes", ctypes.c_uint64), ("slots", ctypes.c_uint32)]
 
 
 class _ScanResult(ctypes.Structure):
@@ -135,6 +151,15 @@ def load_library(path=LIB_PATH):
         "ffbf_batch_last_error": (ctypes.c_char_p, [vp]),
         "ffbf_batch_destroy": (None, [vp]),
         "ffbf_autotune": (ctypes.c_int, [vp, vp, sz, P(ctypes.c_int), P(ctypes.c_int)]),
+        "ffbf_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, P(vp)]),
+        "ffbf_server_add_set": (ctypes.c_int, [vp, vp, P(ctypes.c_uint32)]),
+        "ffbf_server_submit": (ctypes.c_int, [vp, ctypes.c_uint32, vp, sz, P(ctypes.c_uint64)]),
+        "ffbf_server_poll": (ctypes.c_int, [vp, P(_RequestResult), ctypes.c_uint32, P(ctypes.c_uint32),
+                                            ctypes.c_uint32]),
+        "ffbf_server_release": (ctypes.c_int, [vp, ctypes.c_uint64]),
+        "ffbf_server_get_stats": (ctypes.c_int, [vp, P(_ServerStats)]),
+        "ffbf_server_last_error": (ctypes.c_char_p, [vp]),
+        "ffbf_server_destroy": (None, [vp]),
     }
     for name, (res, args) in sig.items():
         fn = getattr(lib, name)
@@ -380,6 +405,98 @@ class Batch:
         if getattr(self, "_h", None):
             self._lib.ffbf_batch_destroy(self._h)
             self._h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *exc):
+        self.close()
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+@dataclass
+class RequestResult:
+    """One finished server request: its hits and candidate lines (as Filter.process returns them) and the
+    server's timestamps (seconds since the server started)."""
+    request_id: int
+    set_id: int
+    status: int
+    text_len: int
+    hit_offsets: np.ndarray
+    line_start: np.ndarray
+    line_end: np.ndarray
+    t_submit: float
+    t_admit: float
+    t_launch: float
+    t_done: float
+
+    @property
+    def latency(self):
+        return self.t_done - self.t_submit
+
+
+class Server:
+    """Scan server (ffbf_server_*): resident pattern sets, admission by free slots and text-arena room,
+    continuous batching of the admitted requests on one GPU."""
+
+    def __init__(self, device=0, arena_bytes=0, slots=0):
+        self._lib = load_library()
+        h = ctypes.c_void_p()
+        st = self._lib.ffbf_server_create(device, arena_bytes, slots, ctypes.byref(h))
+        if st != 0:
+            raise FFBFError(st, "ffbf_server_create failed")
+        self._h = h
+        self._texts = {}  # request id -> the submitted buffer, kept alive until the request is polled
+        self._sets = []
+
+    def _check(self, st):
+        if st != 0:
+            raise FFBFError(st, self._lib.ffbf_server_last_error(self._h).decode(errors="replace"))
+
+    def add_set(self, filt):
+        sid = ctypes.c_uint32()
+        self._check(self._lib.ffbf_server_add_set(self._h, filt._h, ctypes.byref(sid)))
+        self._sets.append(filt)
+        return sid.value
+
+    def submit(self, set_id, text):
+        """Queues a scan of `text` (a uint8 numpy array, ideally in pinned memory) against a set."""
+        a = np.ascontiguousarray(text, dtype=np.uint8)
+        rid = ctypes.c_uint64()
+        self._check(self._lib.ffbf_server_submit(self._h, set_id, a.ctypes.data_as(ctypes.c_void_p), a.size,
+                                                 ctypes.byref(rid)))
+        self._texts[rid.value] = a
+        return rid.value
+
+    def poll(self, max_results=256, wait_us=0):
+        out = (_RequestResult * max_results)()
+        n = ctypes.c_uint32()
+        self._check(self._lib.ffbf_server_poll(self._h, out, max_results, ctypes.byref(n), wait_us))
+        res = []
+        for i in range(n.value):
+            r = out[i]
+            res.append(RequestResult(int(r.request_id), int(r.set_id), int(r.status), int(r.text_len),
+                                     _arr(r.hit_offsets, r.n_hits), _arr(r.line_start, r.n_lines),
+                                     _arr(r.line_end, r.n_lines), r.t_submit, r.t_admit, r.t_launch, r.t_done))
+            self._lib.ffbf_server_release(self._h, r.request_id)
+            self._texts.pop(int(r.request_id), None)
+        return res
+
+    def stats(self):
+        s = _ServerStats()
+        self._check(self._lib.ffbf_server_get_stats(self._h, ctypes.byref(s)))
+        return {f: getattr(s, f) for f, _ in _ServerStats._fields_}
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.ffbf_server_destroy(self._h)
+            self._h = None
+            self._texts.clear()
 
     def __enter__(self):
         return self

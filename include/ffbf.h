@@ -192,6 +192,53 @@ void* ffbf_batch_stream(ffbf_batch* b);
 const char* ffbf_batch_last_error(const ffbf_batch* b);
 void ffbf_batch_destroy(ffbf_batch* b);
 
+/* Scan server: pattern sets resident on the device, scan requests admitted while device memory allows,
+ * and every admitted request whose text has reached the device scanned together in the next launch
+ * sequence (continuous batching). The reference has no counterpart: it scans one corpus per process
+ * (ffbf.cpp:529-601); a request here produces what ffbf_scan would for its text and set.
+ *
+ * ffbf_server_create reserves `arena_bytes` of device memory for request texts (0: half the device's free
+ * memory) and `slots` request slots (0: 64), then starts a host thread that runs the loop: admit requests
+ * in arrival order while a slot and arena room are free, copy each text to the arena on a copy stream,
+ * launch every request whose copy has finished as soon as the previous launch sequence is done, and
+ * collect each finished request's hits and lines (the line resolution of one batch overlaps the next
+ * batch's scan). A request's feed-forward bits go into its set's filter, as successive ffbf_scan calls on
+ * the set would.
+ *
+ * Register sets with ffbf_server_add_set before the first submit (the server borrows the context's filters;
+ * the context must not be modified or used for other calls until the server is destroyed). A submitted
+ * text must stay valid until the request is polled; pinned host memory lets its copy overlap other work.
+ * ffbf_server_poll returns finished requests (waiting up to wait_us microseconds for the first one);
+ * their arrays stay valid until ffbf_server_release. Times are seconds since the server's creation,
+ * from the host's steady clock. A request longer than the arena is refused with FFBF_EINVAL. */
+typedef struct ffbf_server ffbf_server;
+typedef struct {
+    uint64_t request_id;
+    uint32_t set_id;
+    ffbf_status status;
+    uint64_t text_len;
+    uint64_t n_hits;
+    const uint64_t* hit_offsets; /* ascending */
+    uint64_t n_lines;
+    const uint64_t* line_start;  /* candidate lines, as ffbf_scan_result */
+    const uint64_t* line_end;
+    double t_submit, t_admit, t_launch, t_done;
+} ffbf_request_result;
+typedef struct {
+    uint64_t requests_done, batches, bytes_scanned, max_batch;
+    uint64_t arena_bytes;
+    uint32_t slots;
+} ffbf_server_stats;
+ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots, ffbf_server** out);
+ffbf_status ffbf_server_add_set(ffbf_server* s, ffbf_ctx* set, uint32_t* set_id);
+ffbf_status ffbf_server_submit(ffbf_server* s, uint32_t set_id, const uint8_t* text, size_t len, uint64_t* request_id);
+ffbf_status ffbf_server_poll(ffbf_server* s, ffbf_request_result* out, uint32_t max, uint32_t* n_out,
+                             uint32_t wait_us);
+ffbf_status ffbf_server_release(ffbf_server* s, uint64_t request_id);
+ffbf_status ffbf_server_get_stats(ffbf_server* s, ffbf_server_stats* out);
+const char* ffbf_server_last_error(const ffbf_server* s);
+void ffbf_server_destroy(ffbf_server* s);  /* waits for work on the device; unfinished requests are dropped */
+
 /* Autotuner: times the tuned scan's configurations (CTA size, shared-memory vs L2 filter placement) on the
  * first `sample_len` bytes of a device text with this context's filter, keeps the fastest for later scans
  * of the context, and reports it (threads, mode: 0 shared-memory stage, 1 pipelined L2 probes). The
