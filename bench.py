@@ -44,10 +44,13 @@ def parse():
     ap.add_argument("--steps", type=int, default=10)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", choices=["ours", "reference"], default="ours")
-    ap.add_argument("--workload", choices=["scale", "plain", "binary", "batched"], default="scale")
+    ap.add_argument("--workload", choices=["scale", "plain", "binary", "batched", "served"], default="scale")
     ap.add_argument("--batch-jobs", type=int, default=512, help="jobs of the batched workload")
     ap.add_argument("--batch-max-text", type=int, default=256 << 20, help="largest job text of the batched workload")
     ap.add_argument("--no-batched", action="store_true", help="skip the batched leg of the default run")
+    ap.add_argument("--no-served", action="store_true", help="skip the served leg of the default run")
+    ap.add_argument("--served-requests", type=int, default=4000, help="requests of the served workload")
+    ap.add_argument("--served-rate", type=float, default=2000.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--text-bytes", type=int, default=0, help="override the workload's text size")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (default: min(steps, 5))")
@@ -415,6 +418,150 @@ def run_batched(args, local):
     return out
 
 
+# ---- served form: resident sets, Poisson arrivals, continuous batching vs serial plain calls ------------
+def served_trace(n, rate, seed, n_sets, pool_bytes):
+    """(arrival s, set, offset, length) per request: Poisson arrivals, sets uniform, sizes log-normal
+    (median 1 MiB, sigma 1.5, capped at 512 MiB), 256-byte aligned offsets into the text pool."""
+    rng = np.random.default_rng(seed ^ 0x5E4BED)
+    arrivals = np.cumsum(rng.exponential(1.0 / rate, n))
+    sets = rng.integers(0, n_sets, n)
+    sizes = np.minimum(np.exp(np.log(1 << 20) + 1.5 * rng.standard_normal(n)), 512 << 20).astype(np.int64)
+    sizes = np.maximum(sizes, 1)
+    offs = (rng.integers(0, pool_bytes - sizes + 1) // 256 * 256).astype(np.int64)
+    return [(float(a), int(si), int(o), int(z)) for a, si, o, z in zip(arrivals, sets, offs, sizes)]
+
+
+def wait_until(start, t):
+    """Sleeps, then spins, until t seconds after start (sleeping releases the GIL for other threads)."""
+    while True:
+        dt = t - (time.perf_counter() - start)
+        if dt <= 0:
+            return
+        if dt > 5e-4:
+            time.sleep(dt - 3e-4)
+
+
+def pct(xs, q):
+    return float(np.percentile(np.asarray(xs), q)) if len(xs) else None
+
+
+def run_served(args, local):
+    """The served workload through ffbf_server_* and through serial plain ffbf_scan calls.
+
+    8 resident sets of 100k-1M printable patterns (32-64 B, LEN 32, the scale workload's geometry); one
+    1 GiB pinned pool of printable text ('\\n' after geometric(mean 100) bytes) with occurrences of every
+    set planted, from which each request takes a slice. Runs: `served` at the Poisson rate (latency =
+    server's done - submit time), `served_saturated` with every request submitted at once (capacity),
+    `plain_serial` = one ffbf_scan call per request in arrival order, paced by the same arrival times
+    (latency includes waiting for the previous call), and its unpaced capacity. All from host memory:
+    every request's bytes cross PCIe in every run.
+    """
+    import threading
+
+    import torch
+
+    from ffbf_b200 import Filter, Server
+    from ffbf_b200 import datagen as dg
+
+    n_sets, pool_bytes = 8, 1 << 30
+    rng = np.random.default_rng(args.seed ^ 0x5E7)
+    counts = rng.integers(100_000, 1_000_001, n_sets)
+    prm = dg.scale().params
+    t0 = time.perf_counter()
+    pats = [dg.gen_patterns(args.seed + 100 + i, dg.PRINTABLE, int(c), 32, 64) for i, c in enumerate(counts)]
+    host = torch.empty(pool_bytes, dtype=torch.uint8, pin_memory=True)
+    pool = host.numpy()
+    dg.gen_text(args.seed + 99, dg.PRINTABLE, pool_bytes, 100, out=pool)
+    for i, pb in enumerate(pats):
+        dg.plant(args.seed + 200 + i, pb, pool, 2000)
+    filters = []
+    for pb in pats:
+        f = Filter(prm, device=local)
+        f.add_patterns(pb)
+        filters.append(f)
+    torch.cuda.synchronize()
+    setup_s = time.perf_counter() - t0
+    trace = served_trace(args.served_requests, args.served_rate, args.seed, n_sets, pool_bytes)
+    total = sum(z for _, _, _, z in trace)
+
+    # serial plain calls: paced by the arrival times, then back to back
+    def plain(paced):
+        for f in filters:
+            f.clear_ff()
+        lat, res = [], []
+        start = time.perf_counter()
+        for a, si, o, z in trace:
+            if paced:
+                wait_until(start, a)
+            r = filters[si].process(pool[o:o + z])
+            done = time.perf_counter() - start
+            lat.append(done - (a if paced else 0.0))
+            res.append((r.hit_offsets.copy(), r.line_start.copy()))
+        return lat, res, time.perf_counter() - start, [ff_digest(f) for f in filters]
+
+    # the unpaced pass first: it also grows every context's buffers to the largest request
+    _, _, plain_cap_span, _ = plain(False)
+    plain_lat, plain_res, plain_span, plain_ff = plain(True)
+
+    def served(paced):
+        for f in filters:
+            f.clear_ff()
+        torch.cuda.synchronize()
+        srv = Server(local, arena_bytes=16 << 30, slots=64)
+        sids = [srv.add_set(f) for f in filters]
+        ids = [None] * len(trace)
+
+        def submitter():
+            start = time.perf_counter()
+            for i, (a, si, o, z) in enumerate(trace):
+                if paced:
+                    wait_until(start, a)
+                ids[i] = srv.submit(sids[si], pool[o:o + z])
+
+        th = threading.Thread(target=submitter)
+        th.start()
+        got = {}
+        while len(got) < len(trace):
+            for r in srv.poll(max_results=512, wait_us=2000):
+                got[r.request_id] = r
+        th.join()
+        st = srv.stats()
+        srv.close()
+        out = [got[i] for i in ids]
+        span = max(r.t_done for r in out) - min(r.t_submit for r in out)
+        return out, span, st, [ff_digest(f) for f in filters]
+
+    srv_res, srv_span, srv_stats, srv_ff = served(True)
+    _, sat_span, sat_stats, _ = served(False)
+    lat = [r.latency for r in srv_res]
+    exact = all(r.status == 0 and np.array_equal(r.hit_offsets, p[0]) and np.array_equal(r.line_start, p[1])
+                for r, p in zip(srv_res, plain_res)) and srv_ff == plain_ff
+    out = {
+        "workload": f"served: {n_sets} resident sets of {int(counts.min())}-{int(counts.max())} printable "
+                    f"patterns (32-64 B, LEN 32, K 5, S 2, 2^23+2^26 bits); {len(trace)} requests, Poisson "
+                    f"{args.served_rate:g}/s, sizes log-normal (median 1 MiB, sigma 1.5, cap 512 MiB), "
+                    f"{total / 2**30:.2f} GiB in all, slices of a 1 GiB pinned host pool",
+        "requests": len(trace), "text_bytes": total, "offered_gbs": total / trace[-1][0] / 1e9,
+        "served": {"p50_ms": pct(lat, 50) * 1e3, "p99_ms": pct(lat, 99) * 1e3, "gbs": total / srv_span / 1e9,
+                   "batches": srv_stats["batches"], "max_batch": srv_stats["max_batch"],
+                   "mean_batch": len(trace) / max(srv_stats["batches"], 1)},
+        "served_saturated": {"gbs": total / sat_span / 1e9, "batches": sat_stats["batches"],
+                             "max_batch": sat_stats["max_batch"]},
+        "plain_serial": {"p50_ms": pct(plain_lat, 50) * 1e3, "p99_ms": pct(plain_lat, 99) * 1e3,
+                         "gbs": total / plain_span / 1e9, "capacity_gbs": total / plain_cap_span / 1e9},
+        "served_over_plain_capacity": plain_cap_span / sat_span,
+        "bit_exact_vs_plain": bool(exact),
+        "setup_s": setup_s,
+        "timing": "host steady clock; served latency = done - submit inside the server; plain latency = done - "
+                  "arrival; every run copies each request's text from pinned host memory",
+    }
+    for f in filters:
+        f.close()
+    del host
+    torch.cuda.empty_cache()
+    return out
+
+
 # ---- our arm --------------------------------------------------------------------------------------------
 def main_ours(args):
     import torch
@@ -445,6 +592,8 @@ def main_ours(args):
 
     if args.workload == "batched":
         return main_batched(args, world, rank, local, barrier, max_over_ranks)
+    if args.workload == "served":
+        return main_served(args, world, rank, local, barrier, max_over_ranks)
 
     wl = workload(args)
     seed = args.seed + rank  # independent replicas
@@ -537,6 +686,8 @@ def main_ours(args):
     if world == 1 and args.workload == "scale" and not args.no_batched:
         # the batched form against plain per-job launches (its own workload, same GPU)
         line["batched"] = run_batched(args, local)
+    if world == 1 and args.workload == "scale" and not args.no_served:
+        line["served"] = run_served(args, local)
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:
@@ -566,6 +717,30 @@ def main_batched(args, world, rank, local, barrier, max_over_ranks):
                          "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
                          "algorithmic_bytes_per_launch": r["text_bytes"]},
             "gpu_launches": r["launches_per_step"]["batched"] * args.steps, "clocks": clocks, "batched": r}
+    if world > 1:
+        dist.destroy_process_group()
+    if rank == 0:
+        print(json.dumps(line))
+    return 0
+
+
+def main_served(args, world, rank, local, barrier, max_over_ranks):
+    """Headline line for the served workload: value = GB/s at the Poisson rate, with p50/p99 latency."""
+    import torch.distributed as dist
+
+    sampler = ClockSampler(gpu_id_for(local))
+    sampler.start()
+    barrier()
+    r = run_served(args, local)
+    clocks = sampler.stop()
+    line = {"metric": "served GB/s and p50/p99 latency", "value": world * r["served"]["gbs"], "unit": UNIT,
+            "n_gpus": world, "steps": 1, "warmup": 0, "ms_per_step": None, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic",
+            "config": {"workload": r["workload"], "l2": "request texts stream from host memory",
+                       "parallelism": f"replicas x{world}" if world > 1 else "single GPU"},
+            "e2e": {"value": world * r["served"]["gbs"], "unit": UNIT, "h2d_bytes_per_step": r["text_bytes"],
+                    "d2h_bytes_per_step": None},
+            "clocks": clocks, "served": r}
     if world > 1:
         dist.destroy_process_group()
     if rank == 0:

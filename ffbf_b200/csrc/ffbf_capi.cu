@@ -132,6 +132,24 @@ ffbf_status to_host_buffer(ffbf_ctx* c, const std::vector<uint8_t>& v, uint8_t**
     return FFBF_OK;
 }
 
+void order_hits(const HitRec* hr, const HitLine* hl, uint32_t nh, std::vector<uint64_t>& hits,
+                std::vector<uint64_t>& ls, std::vector<uint64_t>& le) {
+    std::vector<uint32_t> order(nh);
+    for (uint32_t i = 0; i < nh; i++) order[i] = i;
+    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return hr[a].off < hr[b].off; });
+    hits.resize(nh);
+    ls.clear();
+    le.clear();
+    for (uint32_t i = 0; i < nh; i++) {
+        const uint32_t j = order[i];
+        hits[i] = hr[j].off;
+        if (ls.empty() || ls.back() != hl[j].start) {
+            ls.push_back(hl[j].start);
+            le.push_back(hl[j].end);
+        }
+    }
+}
+
 void reset_scan(ffbf_ctx* c) {
     c->have_scan = false;
     c->scan_pending = false;
@@ -632,20 +650,7 @@ ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
             CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->d_hitlines, nh * sizeof(HitLine), cudaMemcpyDeviceToHost, c->st));
         }
         TRY(sync(c));
-        std::vector<uint32_t> order(nh);
-        for (uint32_t i = 0; i < nh; i++) order[i] = i;
-        std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) { return hr[a].off < hr[b].off; });
-        c->r_hits.resize(nh);
-        c->r_ls.clear();
-        c->r_le.clear();
-        for (uint32_t i = 0; i < nh; i++) {
-            const uint32_t j = order[i];
-            c->r_hits[i] = hr[j].off;
-            if (c->r_ls.empty() || c->r_ls.back() != hl[j].start) {
-                c->r_ls.push_back(hl[j].start);
-                c->r_le.push_back(hl[j].end);
-            }
-        }
+        order_hits(hr.data(), hl.data(), nh, c->r_hits, c->r_ls, c->r_le);
         c->scan_pending = false;
         c->have_scan = true;
     }

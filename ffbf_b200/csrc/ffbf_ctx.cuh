@@ -137,6 +137,9 @@ void dfree(ffbf_ctx* c, T*& p) {
 ffbf_status enter(ffbf_ctx* c);  // clears the last error and makes the context's device current
 ffbf_status sync(ffbf_ctx* c);   // waits for the context's stream
 void reset_scan(ffbf_ctx* c);    // forgets the last scan's results
+// Hit windows in text order and their lines, each line once (the hits come in any order).
+void order_hits(const HitRec* hr, const HitLine* hl, uint32_t nh, std::vector<uint64_t>& hits,
+                std::vector<uint64_t>& ls, std::vector<uint64_t>& le);
 // Stage-1 table and probe mode of the tuned scan for the context's filter (no-op for borrowed filters).
 ffbf_status prepare_fast(ffbf_ctx* c);
 ffbf::ScanArgs make_scan_args(ffbf_ctx* c);

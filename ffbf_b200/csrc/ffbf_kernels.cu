@@ -346,6 +346,19 @@ cudaError_t zero_counters(uint32_t* const* d_ptrs, uint32_t n, cudaStream_t st) 
     return cudaGetLastError();
 }
 
+// Copies the counters of n jobs into one array (CNT_WORDS words per job), for one device-to-host copy.
+__global__ void k_gather_counters(uint32_t* const* ptrs, uint32_t n, uint32_t* out) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n * CNT_WORDS) out[i] = ptrs[i / CNT_WORDS][i % CNT_WORDS];
+}
+
+cudaError_t gather_counters(uint32_t* const* d_ptrs, uint32_t n, uint32_t* d_out, cudaStream_t st) {
+    if (!n) return cudaSuccess;
+    k_gather_counters<<<(n * CNT_WORDS + 255) / 256, 256, 0, st>>>(d_ptrs, n, d_out);
+    note_launches(1);
+    return cudaGetLastError();
+}
+
 int scan_generic_grid(const Geom& g, int cache_in_smem, uint64_t ntiles) {
     size_t smem = scan_smem_bytes(cache_in_smem, g);
     if (cudaFuncSetAttribute(k_scan_generic, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem) != cudaSuccess)

@@ -73,6 +73,7 @@ int scan_generic_grid(const Geom& g, int cache_in_smem, uint64_t ntiles);
 cudaError_t scan_generic_multi(const ScanArgs* d_jobs, const uint2* d_items, uint32_t n_items, int num_sms,
                                cudaStream_t st);
 cudaError_t zero_counters(uint32_t* const* d_ptrs, uint32_t n, cudaStream_t st);
+cudaError_t gather_counters(uint32_t* const* d_ptrs, uint32_t n, uint32_t* d_out, cudaStream_t st);
 cudaError_t scan_generic(const ScanArgs& a, int grid, cudaStream_t st);
 cudaError_t resolve_lines(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
                           const long long* tile_first, const long long* tile_last, long long* prev_nl,

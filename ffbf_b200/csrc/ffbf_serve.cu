@@ -9,8 +9,10 @@
 //   4. when the previous launch sequence has finished, launches every ready request as one plan
 //      (build_plan/launch_plan: one tuned launch per (LEN, configuration) group, one generic launch for
 //      ragged ends) on the scan stream;
-//   5. collects one finished request: line resolution and the copy of its hits on the slot's own stream,
-//      which overlaps the next batch's scan; then frees its slot and arena range.
+//   5. for each request of a finished batch (whose hit counts came back with the batch), enqueues line
+//      resolution and the copy of its hits on the slot's own stream, overlapping the next batch's scan;
+//      a request whose copy has landed is ordered on the host and its slot and arena range are freed.
+//      A request with more hits than its slot's buffer takes the plain collect (regrow and rescan).
 // A slot is a context with its own scan buffers whose filters are attached from the request's set.
 #include <cuda_runtime.h>
 
@@ -43,6 +45,7 @@ struct Request {
     uint64_t off = 0;
     uint64_t span = 0;  // arena bytes held
     int slot = -1;
+    uint32_t nh = 0;  // hit windows, read back with the batch
     double t_submit = 0, t_admit = 0, t_launch = 0, t_done = 0;
     ffbf_status status = FFBF_OK;
     std::vector<uint64_t> hits, ls, le;
@@ -81,6 +84,15 @@ struct ffbf_server {
     uint32_t** h_counters = nullptr;
     uint2* h_tail = nullptr;
     uint32_t* h_ctl = nullptr;  // error flags read back after each batch
+    uint32_t* d_cnt = nullptr;  // every job's counters, gathered after each batch
+    uint32_t* h_cnt = nullptr;
+    struct SlotHost {
+        HitRec* hr = nullptr;  // pinned copies of the slot's hit records and lines
+        HitLine* hl = nullptr;
+        uint32_t cap = 0;
+        cudaEvent_t done = nullptr;
+    };
+    std::vector<SlotHost> slot_host;
     cudaEvent_t batch_done = nullptr;
     uint32_t batch_ctl = 0;
 
@@ -98,7 +110,7 @@ struct ffbf_server {
 
     // worker-only state
     std::deque<Request*> pending;
-    std::vector<Request*> copying, ready, running, collect;
+    std::vector<Request*> copying, ready, running, resolving, slow;
     bool in_flight = false;
 
     double now() const { return std::chrono::duration<double>(Clock::now() - t0).count(); }
@@ -235,6 +247,9 @@ void launch_ready(ffbf_server* s) {
     up(s->d_counters, s->h_counters, (n + n_ctl) * sizeof(uint32_t*));
     const double t = s->now();
     if (e == cudaSuccess) e = launch_plan(plan, d, s->num_sms, s->st_scan);
+    if (e == cudaSuccess) e = ffbf::gather_counters(s->d_counters, n, s->d_cnt, s->st_scan);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(s->h_cnt, s->d_cnt, 4 * ffbf::CNT_WORDS * n, cudaMemcpyDeviceToHost, s->st_scan);
     if (e == cudaSuccess)
         e = cudaMemcpyAsync(s->h_ctl, s->d_ctl, 16 * n_ctl, cudaMemcpyDeviceToHost, s->st_scan);
     if (e == cudaSuccess) e = cudaEventRecord(s->batch_done, s->st_scan);
@@ -253,9 +268,10 @@ void launch_ready(ffbf_server* s) {
     s->stats.max_batch = std::max<uint64_t>(s->stats.max_batch, n);
 }
 
-void collect_one(ffbf_server* s) {
-    Request* r = s->collect.front();
-    s->collect.erase(s->collect.begin());
+// The plain collect: waits on the slot's stream, grows the hit buffer and rescans when needed.
+void collect_slow(ffbf_server* s) {
+    Request* r = s->slow.front();
+    s->slow.erase(s->slow.begin());
     ffbf_ctx* slot = s->slots[r->slot];
     ffbf_scan_result res{};
     ffbf_status st = ffbf_scan_collect(slot, &res);
@@ -269,13 +285,73 @@ void collect_one(ffbf_server* s) {
     finish(s, r, st);
 }
 
+// Enqueues line resolution and the copy of the hit records for a request of a finished batch.
+ffbf_status start_resolve(ffbf_server* s, Request* r) {
+    ffbf_ctx* c = s->slots[r->slot];
+    auto& h = s->slot_host[r->slot];
+    const uint32_t nh = r->nh;
+    if (nh > h.cap) {
+        if (h.hr) cudaFreeHost(h.hr);
+        if (h.hl) cudaFreeHost(h.hl);
+        h.hr = nullptr;
+        h.hl = nullptr;
+        h.cap = 0;
+        const uint32_t cap = std::max<uint32_t>(nh, 4096);
+        if (cudaMallocHost(&h.hr, cap * sizeof(HitRec)) != cudaSuccess ||
+            cudaMallocHost(&h.hl, cap * sizeof(HitLine)) != cudaSuccess) {
+            cudaGetLastError();
+            return FFBF_ENOMEM_HOST;
+        }
+        h.cap = cap;
+    }
+    const uint64_t ntiles = (c->text_len + ffbf::kScanTile - 1) / ffbf::kScanTile;
+    cudaError_t e = ffbf::resolve_lines(c->d_text, c->text_len, c->g.len, c->d_hits, nh, c->d_tiles,
+                                        c->d_tiles + c->tiles_cap, c->d_tiles + 2 * c->tiles_cap,
+                                        c->d_tiles + 3 * c->tiles_cap, ntiles, c->d_hitlines, c->st);
+    if (e == cudaSuccess && nh)
+        e = cudaMemcpyAsync(h.hr, c->d_hits, nh * sizeof(HitRec), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess && nh)
+        e = cudaMemcpyAsync(h.hl, c->d_hitlines, nh * sizeof(HitLine), cudaMemcpyDeviceToHost, c->st);
+    if (e == cudaSuccess) e = cudaEventRecord(h.done, c->st);
+    if (e != cudaSuccess) {
+        cudaGetLastError();
+        s->err = std::string("result copy failed: ") + cudaGetErrorString(e);
+        return FFBF_ECUDA;
+    }
+    return FFBF_OK;
+}
+
+// Finishes the requests whose result copies have landed.
+bool finish_resolved(ffbf_server* s) {
+    bool any = false;
+    for (size_t i = 0; i < s->resolving.size();) {
+        Request* r = s->resolving[i];
+        auto& h = s->slot_host[r->slot];
+        const cudaError_t q = cudaEventQuery(h.done);
+        if (q == cudaErrorNotReady) {
+            i++;
+            continue;
+        }
+        s->resolving.erase(s->resolving.begin() + i);
+        if (q == cudaSuccess) {
+            order_hits(h.hr, h.hl, r->nh, r->hits, r->ls, r->le);
+            finish(s, r, FFBF_OK);
+        } else {
+            cudaGetLastError();
+            finish(s, r, FFBF_ECUDA);
+        }
+        any = true;
+    }
+    return any;
+}
+
 void worker_loop(ffbf_server* s) {
     cudaSetDevice(s->device);
     for (;;) {
         {
             std::unique_lock<std::mutex> lk(s->mu);
             const bool idle = s->pending.empty() && s->copying.empty() && s->ready.empty() && !s->in_flight &&
-                              s->collect.empty();
+                              s->resolving.empty() && s->slow.empty();
             if (idle && s->inbox.empty() && !s->stop) s->cv_work.wait_for(lk, std::chrono::milliseconds(5));
             while (!s->inbox.empty()) {
                 s->pending.push_back(s->inbox.front());
@@ -311,11 +387,26 @@ void worker_loop(ffbf_server* s) {
                 for (uint32_t i = 0; i < s->batch_ctl; i++) flags |= s->h_ctl[4 * i];
                 const ffbf_status st = q != cudaSuccess ? FFBF_ECUDA : flags & 4u ? FFBF_ETIMEOUT : flags ? FFBF_ECUDA : FFBF_OK;
                 if (q != cudaSuccess) cudaGetLastError();
-                for (Request* r : s->running) {
-                    if (st == FFBF_OK) s->collect.push_back(r);
-                    else finish(s, r, st);
+                std::vector<Request*> done_batch;
+                done_batch.swap(s->running);
+                // hit counts first: the next batch's readback reuses the pinned buffer
+                for (size_t i = 0; i < done_batch.size(); i++)
+                    done_batch[i]->nh = s->h_cnt[ffbf::CNT_WORDS * i + ffbf::CNT_HITS];
+                // the GPU is idle: start the next batch before resolving this one's results
+                if (!s->ready.empty()) launch_ready(s);
+                for (Request* r : done_batch) {
+                    if (st != FFBF_OK) {
+                        finish(s, r, st);
+                        continue;
+                    }
+                    if (r->nh > s->slots[r->slot]->hits_cap) {
+                        s->slow.push_back(r);
+                        continue;
+                    }
+                    const ffbf_status rs = start_resolve(s, r);
+                    if (rs == FFBF_OK) s->resolving.push_back(r);
+                    else finish(s, r, rs);
                 }
-                s->running.clear();
                 progress = true;
             }
         }
@@ -323,8 +414,9 @@ void worker_loop(ffbf_server* s) {
             launch_ready(s);
             progress = true;
         }
-        if (!s->collect.empty()) {
-            collect_one(s);
+        progress |= finish_resolved(s);
+        if (!s->slow.empty()) {
+            collect_slow(s);
             progress = true;
         }
         if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(10));
@@ -340,11 +432,17 @@ void server_free(ffbf_server* s) {
     cudaSetDevice(s->device);
     for (auto* c : s->slots) ffbf_destroy(c);
     for (auto ev : s->copy_done) cudaEventDestroy(ev);
+    for (auto& h : s->slot_host) {
+        if (h.hr) cudaFreeHost(h.hr);
+        if (h.hl) cudaFreeHost(h.hl);
+        if (h.done) cudaEventDestroy(h.done);
+    }
     if (s->batch_done) cudaEventDestroy(s->batch_done);
     for (void* p : {(void*)s->d_arena, (void*)s->d_fast, (void*)s->d_args, (void*)s->d_counters, (void*)s->d_ctl,
-                    (void*)s->d_tail})
+                    (void*)s->d_tail, (void*)s->d_cnt})
         if (p) cudaFree(p);
-    for (void* p : {(void*)s->h_fast, (void*)s->h_args, (void*)s->h_counters, (void*)s->h_tail, (void*)s->h_ctl})
+    for (void* p : {(void*)s->h_fast, (void*)s->h_args, (void*)s->h_counters, (void*)s->h_tail, (void*)s->h_ctl,
+                    (void*)s->h_cnt})
         if (p) cudaFreeHost(p);
     if (s->st_scan) cudaStreamDestroy(s->st_scan);
     if (s->st_copy) cudaStreamDestroy(s->st_copy);
@@ -355,7 +453,7 @@ void server_free(ffbf_server* s) {
     drop(s->inbox);
     drop(s->pending);
     drop(s->done);
-    for (auto* v : {&s->copying, &s->ready, &s->running, &s->collect}) {
+    for (auto* v : {&s->copying, &s->ready, &s->running, &s->resolving, &s->slow}) {
         for (auto* r : *v) delete r;
         v->clear();
     }
@@ -407,7 +505,9 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
         cudaMallocHost(&s->h_fast, slots * sizeof(ffbf::FastJob)) != cudaSuccess ||
         cudaMallocHost(&s->h_args, slots * sizeof(ffbf::ScanArgs)) != cudaSuccess ||
         cudaMallocHost(&s->h_counters, n_counters * sizeof(uint32_t*)) != cudaSuccess ||
-        cudaMallocHost(&s->h_ctl, 16 * kMaxCtl) != cudaSuccess || !ensure_tail(s, 4096)) {
+        cudaMallocHost(&s->h_ctl, 16 * kMaxCtl) != cudaSuccess ||
+        cudaMalloc(&s->d_cnt, 4 * ffbf::CNT_WORDS * (size_t)slots) != cudaSuccess ||
+        cudaMallocHost(&s->h_cnt, 4 * ffbf::CNT_WORDS * (size_t)slots) != cudaSuccess || !ensure_tail(s, 4096)) {
         cudaGetLastError();
         return bail(FFBF_ENOMEM_DEVICE);
     }
@@ -422,6 +522,11 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
             return bail(FFBF_ECUDA);
         }
         s->copy_done.push_back(ev);
+        s->slot_host.emplace_back();
+        if (cudaEventCreateWithFlags(&s->slot_host.back().done, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(FFBF_ECUDA);
+        }
         s->free_slots.push_back((int)(slots - 1 - i));
     }
     s->stats.arena_bytes = arena_bytes;

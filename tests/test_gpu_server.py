@@ -2,7 +2,8 @@
 text, whether the request runs alone or batched with requests of other sets; each set's feed-forward filter
 ends as the union of what its requests set, as successive ffbf_scan calls would leave it.
 
-The sets cover the tuned kernel's sparse and dense modes, a geometry only the generic kernel handles, and
+The sets cover the tuned kernel's sparse and dense modes, a geometry only the generic kernel handles, a
+filter so full that a request overflows its slot's hit buffer (the server then grows it and rescans), and
 request sizes from empty through ragged tile ends to several MiB. A small text arena and few slots make
 admission wait for room.
 """
@@ -17,7 +18,7 @@ from ffbf_b200 import FFBFError, Filter, Server
 
 pytestmark = pytest.mark.gpu
 
-SETS = ["scale_small", "plain_small", "smem_cache", "k11_s0_len63"]
+SETS = ["scale_small", "plain_small", "smem_cache", "k11_s0_len63", "hit_flood"]
 
 
 def request_slices(n, seed):
