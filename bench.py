@@ -565,38 +565,25 @@ def run_served(args, local):
 # ---- our arm --------------------------------------------------------------------------------------------
 def main_ours(args):
     import torch
-    import torch.distributed as dist
 
     import ffbf_b200
     from ffbf_b200 import Filter
+    from ffbf_b200.replicas import Replicas
 
-    world = int(os.environ.get("WORLD_SIZE", "1"))
-    rank = int(os.environ.get("RANK", "0"))
     local = int(os.environ.get("LOCAL_RANK", "0"))
     torch.cuda.set_device(local)
     dev = torch.device("cuda", local)
-    if world > 1:
-        from datetime import timedelta
-        dist.init_process_group("nccl", timeout=timedelta(seconds=300), device_id=dev)
-
-    def barrier():
-        if world > 1:
-            dist.barrier()
-
-    def max_over_ranks(x):
-        if world == 1:
-            return x
-        t = torch.tensor([x], dtype=torch.float64, device=dev)
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-        return float(t.item())
+    rep = Replicas.from_env("nccl", device=dev)  # N GPUs: N independent replicas, no data-path collective
+    world, rank = rep.world, rep.rank
+    barrier, max_over_ranks = rep.barrier, rep.max
 
     if args.workload == "batched":
-        return main_batched(args, world, rank, local, barrier, max_over_ranks)
+        return main_batched(args, rep)
     if args.workload == "served":
-        return main_served(args, world, rank, local, barrier, max_over_ranks)
+        return main_served(args, rep)
 
     wl = workload(args)
-    seed = args.seed + rank  # independent replicas
+    seed = rep.seed(args.seed)
     pats = wl.patterns(seed)
     host = torch.empty(wl.text_bytes, dtype=torch.uint8, pin_memory=True)
     text = host.numpy()
@@ -688,23 +675,21 @@ def main_ours(args):
         line["batched"] = run_batched(args, local)
     if world == 1 and args.workload == "scale" and not args.no_served:
         line["served"] = run_served(args, local)
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
     if rank == 0:
         print(json.dumps(line))
     return 0
 
 
-def main_batched(args, world, rank, local, barrier, max_over_ranks):
+def main_batched(args, rep):
     """Headline line for the batched workload: value = device-timed GB/s of one batch launch."""
-    import torch.distributed as dist
-
+    world, rank, local = rep.world, rep.rank, rep.local
     sampler = ClockSampler(gpu_id_for(local))
     sampler.start()
-    barrier()
+    rep.barrier()
     r = run_batched(args, local)
     clocks = sampler.stop()
-    ms = max_over_ranks(r["ms_per_step"]["batched_device"])
+    ms = rep.max(r["ms_per_step"]["batched_device"])
     value = world * r["text_bytes"] / (ms * 1e-3) / 1e9
     achieved = r["text_bytes"] / (ms * 1e-3) / 1e9
     peak, peak_kind = measured_peaks()
@@ -717,20 +702,18 @@ def main_batched(args, world, rank, local, barrier, max_over_ranks):
                          "peak_source": f"{peak_kind} hbm_gbs", "traffic": None,
                          "algorithmic_bytes_per_launch": r["text_bytes"]},
             "gpu_launches": r["launches_per_step"]["batched"] * args.steps, "clocks": clocks, "batched": r}
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
     if rank == 0:
         print(json.dumps(line))
     return 0
 
 
-def main_served(args, world, rank, local, barrier, max_over_ranks):
+def main_served(args, rep):
     """Headline line for the served workload: value = GB/s at the Poisson rate, with p50/p99 latency."""
-    import torch.distributed as dist
-
+    world, rank, local = rep.world, rep.rank, rep.local
     sampler = ClockSampler(gpu_id_for(local))
     sampler.start()
-    barrier()
+    rep.barrier()
     r = run_served(args, local)
     clocks = sampler.stop()
     line = {"metric": "served GB/s and p50/p99 latency", "value": world * r["served"]["gbs"], "unit": UNIT,
@@ -741,8 +724,7 @@ def main_served(args, world, rank, local, barrier, max_over_ranks):
             "e2e": {"value": world * r["served"]["gbs"], "unit": UNIT, "h2d_bytes_per_step": r["text_bytes"],
                     "d2h_bytes_per_step": None},
             "clocks": clocks, "served": r}
-    if world > 1:
-        dist.destroy_process_group()
+    rep.close()
     if rank == 0:
         print(json.dumps(line))
     return 0
