@@ -312,7 +312,7 @@ ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
     uint32_t* saved = nullptr;
     TRY(dalloc_t(c, &saved, c->filter_bytes / 4));
     CUDA_TRY(c, cudaMemcpyAsync(saved, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
-    const ffbf::FastConfig cands[] = {{512, 0, 0}, {384, 0, 0}, {256, 0, 0}, {256, 1, 0}};
+    const ffbf::FastConfig cands[] = {{512, 0, 0}, {384, 0, 0}, {256, 0, 0}, {384, 1, 0}, {256, 1, 0}};
     ffbf::FastConfig best = c->cfg;
     float best_ms = 1e30f;
     cudaEvent_t e0, e1;

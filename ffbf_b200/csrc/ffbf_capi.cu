@@ -180,8 +180,9 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         if (!c->d_job) TRY(dalloc_t(c, &c->d_job, 1));
         return FFBF_OK;
     }
-    // the table is sized for the configured CTA (in the dense mode it only measures the filter's fill)
-    const int sparse_threads = c->cfg.threads;
+    // the table is sized for the configured CTA; in the dense mode it only measures the filter's fill, so
+    // the table already built is kept
+    const int sparse_threads = c->cfg.mode != 0 && c->d_stage1 ? c->stage1_threads : c->cfg.threads;
     if (c->d_stage1 && c->stage1_threads != sparse_threads) {
         dfree(c, c->d_stage1);
         c->stage1_dirty = true;
@@ -208,7 +209,12 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         CUDA_TRY(c, cudaMemcpyAsync(&ones, c->d_popc, sizeof ones, cudaMemcpyDeviceToHost, c->st));
         TRY(sync(c));
         c->stage1_fill = (double)ones / (32.0 * nw);
-        if (!c->cfg_tuned) c->cfg.mode = c->stage1_fill > 0.3 ? 1 : 0;
+        if (!c->cfg_tuned) {
+            c->cfg.mode = c->force_mode >= 0 ? c->force_mode : c->stage1_fill > 0.3 ? 1 : 0;
+            // default CTA sizes (measured best on the 10k- and 1M-pattern workloads): 512 threads for the
+            // shared-memory stage, 384 for dense filters
+            c->cfg.threads = c->threads_env ? c->threads_env : c->cfg.mode != 0 ? 384 : 512;
+        }
         c->stage1_dirty = false;
     }
     if (c->force_mode >= 0) c->cfg.mode = c->force_mode;
@@ -358,7 +364,7 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
         return bail(FFBF_ECUDA);
     }
     const char* th = getenv("FFBF_SCAN_THREADS");
-    if (th && (atoi(th) == 256 || atoi(th) == 384 || atoi(th) == 512)) c->cfg.threads = atoi(th);
+    if (th && (atoi(th) == 256 || atoi(th) == 384 || atoi(th) == 512)) c->cfg.threads = c->threads_env = atoi(th);
     const char* fm = getenv("FFBF_SCAN_MODE");
     if (fm && (fm[0] == '0' || fm[0] == '1')) c->force_mode = fm[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");

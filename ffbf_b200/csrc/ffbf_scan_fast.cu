@@ -198,7 +198,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
     constexpr int kStageBytes = THREADS * kRowBytes;
     constexpr int kQCap = MODE == 0 ? kQueueCap : 2 * kQueueCap;
     constexpr int kQBytes = kQCap * 16;
-    constexpr int kRing = 8;             // dense mode: ring depth per stage (divides 32)
+    // dense mode: ring depth per stage (divides 32); 384-thread CTAs trade depth for warps (more L2 probes
+    // in flight per SM within the register file)
+    constexpr int kRing = THREADS >= 384 ? 4 : 8;
     constexpr int kBox = THREADS > 256 ? THREADS / 2 : THREADS;  // streams per TMA box (<= 256)
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
@@ -565,7 +567,9 @@ cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
 template <int L>
 cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
                        uint32_t max_s1_words, uint32_t* d_ctl, int num_sms, cudaStream_t st) {
-    if (cfg.mode == 1) return launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
+    if (cfg.mode == 1)  // dense: 384 threads (ring depth 4) or 256 (depth 8); 512 would spill
+        return cfg.threads == 256 ? launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
+                                  : launch_cfg<L, 384, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
     switch (cfg.threads) {
         case 256: return launch_cfg<L, 256, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
         case 384: return launch_cfg<L, 384, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
@@ -605,7 +609,10 @@ uint32_t stage1_words_for(const Geom& g, int threads) {
     return (uint32_t)(((uint64_t)g.cache_bits >> stage1_shift_for(g, threads)) / 32);
 }
 
-int config_threads(const FastConfig& cfg) { return cfg.mode == 1 ? 256 : cfg.threads; }
+int config_threads(const FastConfig& cfg) {
+    if (cfg.mode == 1) return cfg.threads == 256 ? 256 : 384;
+    return cfg.threads == 384 || cfg.threads == 512 ? cfg.threads : 256;
+}
 
 uint32_t fast_rows(uint64_t n, int threads, int num_sms, bool batch) {
     const uint64_t tiles_bytes = n / kScanTile * kScanTile;
@@ -638,8 +645,8 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
     job->main_words = a.main_words;
     job->ff_words = a.ff_words;
     job->stage1_words = stage1_words;
-    job->stage1_shift = cfg.mode == 1 ? 0 : stage1_shift_for(a.g, threads);
-    job->stage1_nwords = cfg.mode == 1 ? 0 : (uint32_t)(((uint64_t)a.g.cache_bits >> job->stage1_shift) / 32);
+    job->stage1_shift = cfg.mode != 0 ? 0 : stage1_shift_for(a.g, threads);
+    job->stage1_nwords = cfg.mode != 0 ? 0 : (uint32_t)(((uint64_t)a.g.cache_bits >> job->stage1_shift) / 32);
     job->hits = a.hits;
     job->hits_cap = a.hits_cap;
     job->counters = a.counters;

@@ -30,8 +30,8 @@ struct alignas(64) FastJob {
     uint64_t n_tiles;  // 16 KiB tiles of the text (bounds the newline summary writes)
 };
 
-// How a job is scanned: CTA size (256/384/512; the dense mode always uses 256), probe mode (0: sparse,
-// shared-memory stage 1; 1: dense, pipelined L2 probes), rows per stream (0: chosen from the text size).
+// How a job is scanned: CTA size (256/384/512), probe mode (0: sparse, shared-memory stage 1; 1: dense,
+// pipelined L2 probes), rows per stream (0: chosen from the text size).
 struct FastConfig {
     int threads;
     int mode;

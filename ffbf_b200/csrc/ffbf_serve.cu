@@ -53,6 +53,8 @@ struct Request {
 
 constexpr uint64_t kArenaAlign = 256;
 constexpr uint32_t kMaxCtl = 64;  // control-word groups per plan (one per tuned launch, plus one)
+constexpr uint64_t kPreallocText = 512ull << 20;  // request size the slots' scan buffers start out sized for
+constexpr uint32_t kPreallocHits = 16384;          // hit records each slot's pinned result copy starts with
 
 }  // namespace
 
@@ -511,11 +513,18 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
         cudaGetLastError();
         return bail(FFBF_ENOMEM_DEVICE);
     }
+    // Slots get their scan buffers up front, sized for requests of up to kPreallocText bytes (tile
+    // summaries, 64k hit records, pinned copies for 16k hits), so that serving rarely allocates: an
+    // allocation inside the loop would synchronise the device and stall every request in flight.
+    const uint64_t prealloc_len = std::min<uint64_t>(arena_bytes, kPreallocText);
     for (uint32_t i = 0; i < slots; i++) {
         ffbf_ctx* c = nullptr;
         ffbf_status st = create_scan_slot(device, &c);
         if (st != FFBF_OK) return bail(st);
         s->slots.push_back(c);
+        if ((st = setup_scan_state(c, s->d_arena, prealloc_len)) != FFBF_OK || (st = prepare_fast(c)) != FFBF_OK)
+            return bail(st);
+        reset_scan(c);
         cudaEvent_t ev;
         if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
             cudaGetLastError();
@@ -523,10 +532,14 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
         }
         s->copy_done.push_back(ev);
         s->slot_host.emplace_back();
-        if (cudaEventCreateWithFlags(&s->slot_host.back().done, cudaEventDisableTiming) != cudaSuccess) {
+        auto& h = s->slot_host.back();
+        if (cudaEventCreateWithFlags(&h.done, cudaEventDisableTiming) != cudaSuccess ||
+            cudaMallocHost(&h.hr, kPreallocHits * sizeof(HitRec)) != cudaSuccess ||
+            cudaMallocHost(&h.hl, kPreallocHits * sizeof(HitLine)) != cudaSuccess) {
             cudaGetLastError();
-            return bail(FFBF_ECUDA);
+            return bail(FFBF_ENOMEM_HOST);
         }
+        h.cap = kPreallocHits;
         s->free_slots.push_back((int)(slots - 1 - i));
     }
     s->stats.arena_bytes = arena_bytes;

@@ -179,6 +179,7 @@ SCAN_VARIANTS = [
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "384"},
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "512"},
     {"FFBF_SCAN_MODE": "1"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_THREADS": "256"},
 ]
 
 
