@@ -269,7 +269,8 @@ ffbf_status setup_scan_state(ffbf_ctx* c, const uint8_t* d_text, size_t len) {
     if (c->tiles_cap < ntiles) {
         dfree(c, c->d_tiles);
         c->tiles_cap = 0;
-        TRY(dalloc_t(c, &c->d_tiles, 4 * ntiles));
+        // first, last, prev, next per tile, then the two-pass scan's block aggregates
+        TRY(dalloc_t(c, &c->d_tiles, 4 * ntiles + 2 * ffbf::tile_agg_words(ntiles)));
         c->tiles_cap = ntiles;
     }
     if (!c->d_hits) {
@@ -648,7 +649,8 @@ ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
         const uint64_t ntiles = (c->text_len + ffbf::kScanTile - 1) / ffbf::kScanTile;
         CUDA_TRY(c, ffbf::resolve_lines(c->d_text, c->text_len, c->g.len, c->d_hits, nh, c->d_tiles,
                                         c->d_tiles + c->tiles_cap, c->d_tiles + 2 * c->tiles_cap,
-                                        c->d_tiles + 3 * c->tiles_cap, ntiles, c->d_hitlines, c->st));
+                                        c->d_tiles + 3 * c->tiles_cap, ntiles, c->d_hitlines, c->st,
+                                        c->d_tiles + 4 * c->tiles_cap));
         std::vector<HitRec> hr(nh);
         std::vector<HitLine> hl(nh);
         if (nh) {

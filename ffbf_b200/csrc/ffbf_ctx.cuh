@@ -48,7 +48,7 @@ struct ffbf_ctx {
     ffbf::HitLine* d_hitlines = nullptr;
     uint32_t hits_cap = 0;
     uint32_t nhits = 0;
-    long long* d_tiles = nullptr;  // 4 arrays of tiles_cap: first, last, prev, next
+    long long* d_tiles = nullptr;  // 4 arrays of tiles_cap (first, last, prev, next), then block aggregates
     uint64_t tiles_cap = 0;
     int scan_path = 0;             // 0 = generic, 1 = fast
     uint32_t* d_stage1 = nullptr;  // stage-1 table of the tuned scan (cache copy or its fold)

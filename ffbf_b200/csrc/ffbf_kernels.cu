@@ -413,6 +413,114 @@ __global__ void __launch_bounds__(1024) k_tile_nl_scan(const long long* first, c
     }
 }
 
+// The same prefix max / suffix min in two passes over blocks of kTileAggBlock tiles (4 per thread):
+// k_tile_agg reduces each block, k_tile_scan2 folds the other blocks' aggregates into a carry and scans its
+// block with warp shuffles. Loads are coalesced and every SM takes part.
+__global__ void __launch_bounds__(1024) k_tile_agg(const long long* first, const long long* last, uint64_t nt,
+                                                   long long* agg_first, long long* agg_last) {
+    __shared__ long long s_f[32], s_l[32];
+    const uint64_t t0 = (uint64_t)blockIdx.x * kTileAggBlock;
+    long long f = LLONG_MAX, l = -1;
+    for (uint32_t k = threadIdx.x; k < kTileAggBlock; k += 1024) {
+        const uint64_t t = t0 + k;
+        if (t < nt) {
+            f = min(f, first[t]);
+            l = max(l, last[t]);
+        }
+    }
+    for (int o = 16; o; o >>= 1) {
+        f = min(f, __shfl_xor_sync(0xffffffffu, f, o));
+        l = max(l, __shfl_xor_sync(0xffffffffu, l, o));
+    }
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        s_f[w] = f;
+        s_l[w] = l;
+    }
+    __syncthreads();
+    if (w == 0) {
+        f = s_f[lane];
+        l = s_l[lane];
+        for (int o = 16; o; o >>= 1) {
+            f = min(f, __shfl_xor_sync(0xffffffffu, f, o));
+            l = max(l, __shfl_xor_sync(0xffffffffu, l, o));
+        }
+        if (lane == 0) {
+            agg_first[blockIdx.x] = f;
+            agg_last[blockIdx.x] = l;
+        }
+    }
+}
+
+__global__ void __launch_bounds__(1024) k_tile_scan2(const long long* first, const long long* last, uint64_t nt,
+                                                     const long long* agg_first, const long long* agg_last,
+                                                     uint32_t nb, long long* prev_nl, long long* next_nl) {
+    __shared__ long long s_a[32], s_b[32];
+    const int w = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    const uint32_t b = blockIdx.x;
+    // carries: the last '\n' of all earlier blocks, the first '\n' of all later ones
+    long long cp = -1, cn = LLONG_MAX;
+    for (uint32_t i = threadIdx.x; i < b; i += 1024) cp = max(cp, agg_last[i]);
+    for (uint32_t i = b + 1 + threadIdx.x; i < nb; i += 1024) cn = min(cn, agg_first[i]);
+    for (int o = 16; o; o >>= 1) {
+        cp = max(cp, __shfl_xor_sync(0xffffffffu, cp, o));
+        cn = min(cn, __shfl_xor_sync(0xffffffffu, cn, o));
+    }
+    if (lane == 0) {
+        s_a[w] = cp;
+        s_b[w] = cn;
+    }
+    __syncthreads();
+    cp = s_a[lane];
+    cn = s_b[lane];
+    for (int o = 16; o; o >>= 1) {
+        cp = max(cp, __shfl_xor_sync(0xffffffffu, cp, o));
+        cn = min(cn, __shfl_xor_sync(0xffffffffu, cn, o));
+    }
+    __syncthreads();
+    // this thread's 4 consecutive tiles
+    const uint64_t t0 = (uint64_t)b * kTileAggBlock + 4u * threadIdx.x;
+    long long L[4], F[4];
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        const bool in = t0 + k < nt;
+        L[k] = in ? last[t0 + k] : -1;
+        F[k] = in ? first[t0 + k] : LLONG_MAX;
+    }
+    const long long mx = max(max(L[0], L[1]), max(L[2], L[3]));
+    const long long mn = min(min(F[0], F[1]), min(F[2], F[3]));
+    // exclusive prefix max of mx and exclusive suffix min of mn over the block's threads
+    long long pre = mx, suf = mn;
+    for (int o = 1; o < 32; o <<= 1) {
+        const long long u = __shfl_up_sync(0xffffffffu, pre, o);
+        const long long d = __shfl_down_sync(0xffffffffu, suf, o);
+        if (lane >= o) pre = max(pre, u);
+        if (lane + o < 32) suf = min(suf, d);
+    }
+    if (lane == 31) s_a[w] = pre;  // warp totals
+    if (lane == 0) s_b[w] = suf;
+    __syncthreads();
+    long long wpre = -1, wsuf = LLONG_MAX;
+    for (int u = 0; u < w; u++) wpre = max(wpre, s_a[u]);
+    for (int u = w + 1; u < 32; u++) wsuf = min(wsuf, s_b[u]);
+    long long ex_pre = __shfl_up_sync(0xffffffffu, pre, 1);
+    long long ex_suf = __shfl_down_sync(0xffffffffu, suf, 1);
+    if (lane == 0) ex_pre = -1;
+    if (lane == 31) ex_suf = LLONG_MAX;
+    long long run = max(cp, max(wpre, ex_pre));
+#pragma unroll
+    for (int k = 0; k < 4; k++) {
+        if (t0 + k < nt) prev_nl[t0 + k] = run;
+        run = max(run, L[k]);
+    }
+    run = min(cn, min(wsuf, ex_suf));
+#pragma unroll
+    for (int k = 3; k >= 0; k--) {
+        if (t0 + k < nt) next_nl[t0 + k] = run;
+        run = min(run, F[k]);
+    }
+}
+
 __global__ void k_resolve(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
                           const long long* prev_nl, const long long* next_nl, HitLine* out) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
@@ -440,8 +548,13 @@ __global__ void k_resolve(const uint8_t* text, uint64_t n, uint32_t len, const H
 
 cudaError_t resolve_lines(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
                           const long long* tile_first, const long long* tile_last, long long* prev_nl,
-                          long long* next_nl, uint64_t ntiles, HitLine* out, cudaStream_t st) {
-    if (ntiles) {
+                          long long* next_nl, uint64_t ntiles, HitLine* out, cudaStream_t st, long long* agg) {
+    if (ntiles && agg && ntiles > kTileAggBlock) {
+        const uint32_t nb = (uint32_t)((ntiles + kTileAggBlock - 1) / kTileAggBlock);
+        k_tile_agg<<<nb, 1024, 0, st>>>(tile_first, tile_last, ntiles, agg, agg + nb);
+        k_tile_scan2<<<nb, 1024, 0, st>>>(tile_first, tile_last, ntiles, agg, agg + nb, nb, prev_nl, next_nl);
+        note_launches(2);
+    } else if (ntiles) {
         k_tile_nl_scan<<<1, 1024, 0, st>>>(tile_first, tile_last, prev_nl, next_nl, ntiles);
         note_launches(1);
     }

@@ -75,9 +75,14 @@ cudaError_t scan_generic_multi(const ScanArgs* d_jobs, const uint2* d_items, uin
 cudaError_t zero_counters(uint32_t* const* d_ptrs, uint32_t n, cudaStream_t st);
 cudaError_t gather_counters(uint32_t* const* d_ptrs, uint32_t n, uint32_t* d_out, cudaStream_t st);
 cudaError_t scan_generic(const ScanArgs& a, int grid, cudaStream_t st);
+// Hit -> line span. `agg` (2 * tile_agg_words(ntiles) words, optional) lets the tile-newline scan run
+// over all SMs; without it one block scans the tiles.
+constexpr uint32_t kTileAggBlock = 4096;  // tiles per block of the two-pass tile-newline scan
+inline uint64_t tile_agg_words(uint64_t ntiles) { return ntiles / kTileAggBlock + 1; }
 cudaError_t resolve_lines(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
                           const long long* tile_first, const long long* tile_last, long long* prev_nl,
-                          long long* next_nl, uint64_t ntiles, HitLine* out, cudaStream_t st);
+                          long long* next_nl, uint64_t ntiles, HitLine* out, cudaStream_t st,
+                          long long* agg = nullptr);
 
 cudaError_t prune_flags(const uint64_t* d_start, const uint64_t* d_end, const uint64_t* d_hash, uint64_t npat,
                         const Geom& g, const uint32_t* d_ff, uint8_t* d_flags, cudaStream_t st);

@@ -309,7 +309,8 @@ ffbf_status start_resolve(ffbf_server* s, Request* r) {
     const uint64_t ntiles = (c->text_len + ffbf::kScanTile - 1) / ffbf::kScanTile;
     cudaError_t e = ffbf::resolve_lines(c->d_text, c->text_len, c->g.len, c->d_hits, nh, c->d_tiles,
                                         c->d_tiles + c->tiles_cap, c->d_tiles + 2 * c->tiles_cap,
-                                        c->d_tiles + 3 * c->tiles_cap, ntiles, c->d_hitlines, c->st);
+                                        c->d_tiles + 3 * c->tiles_cap, ntiles, c->d_hitlines, c->st,
+                                        c->d_tiles + 4 * c->tiles_cap);
     if (e == cudaSuccess && nh)
         e = cudaMemcpyAsync(h.hr, c->d_hits, nh * sizeof(HitRec), cudaMemcpyDeviceToHost, c->st);
     if (e == cudaSuccess && nh)

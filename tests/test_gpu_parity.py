@@ -204,3 +204,28 @@ def test_scan_variants_agree_with_oracle(name, monkeypatch):
     monkeypatch.setenv("FFBF_SCAN_THREADS", "0")
     with Filter(prm):
         pass  # restores the default CTA size for later tests
+
+
+def test_line_resolution_over_many_tile_blocks():
+    """Texts above 4096 tiles (64 MiB) resolve lines with the two-pass tile-newline scan: a 100 MiB text with
+    50 KB lines and one 80 MiB line, so a whole block of tiles holds no '\\n' and the line's start and end
+    come from other blocks. Lines, hits and feed-forward bits equal the oracle's."""
+    from ffbf_b200 import datagen as dg
+
+    prm = Params(20, 5, 2, 1 << 24, 1 << 28)
+    pats = dg.gen_patterns(31, dg.PRINTABLE, 2000, 20, 40)
+    text = dg.gen_text(32, dg.PRINTABLE, 100 << 20, 50000)
+    seg = text[10 << 20:90 << 20]
+    seg[seg == 10] = ord("x")
+    dg.plant(33, pats, text, 3000)
+    o = oracle.Oracle.from_params(prm)
+    o.build(pats)
+    s = o.scan(text)
+    assert ((s["line_end"] - s["line_start"]) > (64 << 20)).any()
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        r = f.process(text)
+        np.testing.assert_array_equal(r.hit_offsets, s["hits"])
+        np.testing.assert_array_equal(r.line_start, s["line_start"])
+        np.testing.assert_array_equal(r.line_end, s["line_end"])
+        np.testing.assert_array_equal(f.get_filters()[1], o.ff)
