@@ -166,12 +166,14 @@ __device__ __noinline__ void flush_queue(const FastJob* J, uint32_t qaddr, int q
         const uint64_t h = ((uint64_t)e[t].z << 32) | e[t].y;
         if (!((v[t] >> (bi[t] & 31)) & 1u)) continue;
         if (!full_check_from(g, main_words, h, e[t].w + 1)) continue;
+        // p = window end + 128 relative to the owner's current row (the dense rings carry the previous row's
+        // last windows into the next row)
         const uint32_t owner = e[t].x >> 8, p = e[t].x & 0xFFu;
-        if (owner >= 32 || p >= 128) {
+        if (owner >= 32) {
             atomicOr(counters + CNT_ERROR, 0x400u);
             continue;
         }
-        const uint64_t start = warp_row_pos0 + owner * row_stride + p + 1 - g.len;
+        const uint64_t start = warp_row_pos0 + owner * row_stride + p + 1 - g.len - kRowBytes;
         set_all<2>(g, ff_words, h);
         const uint32_t slot = atomicAdd(counters + CNT_HITS, 1u);
         if (slot < hits_cap) hits[slot] = HitRec{start, h};
@@ -452,13 +454,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                         const bool b0 = (__funnelshift_r(w0, w0, hl) & 1u) != 0;
                         const bool b1 = (__funnelshift_r(w1, w1, hh) & 1u) != 0;
                         const bool pass = active && (j - lnp >= L) && b0 && (b1 || !two);
-                        enqueue(pass, (uint32_t)(32 * b + j), hl, hh, s1_first);
+                        enqueue(pass, (uint32_t)(kRowBytes + 32 * b + j), hl, hh, s1_first);
                     } else {
                         const int slot = j % kRing;
                         // stage B: the window that entered stage A 2*kRing bytes ago
                         // (the second probe's bit sits at h2 & 31 in its word for both index functions)
                         const bool pass2 = (__funnelshift_r(ring2_v[slot], ring2_v[slot], ring2_h[slot]) & 1u) != 0;
-                        enqueue(pass2, (uint32_t)(32 * b + j - 2 * kRing), ring2_l[slot], ring2_h[slot], 2u);
+                        enqueue(pass2, (uint32_t)(kRowBytes + 32 * b + j - 2 * kRing), ring2_l[slot], ring2_h[slot],
+                                2u);
                         // stage A: the window issued kRing bytes ago; its h1 word has arrived by now
                         const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], ring_l[slot]) & 1u) != 0;
                         ring2_l[slot] = ring_l[slot];
@@ -482,16 +485,20 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                 for (int q = 0; q < 8; q++) prev[q] = cur[q];
             }
             if constexpr (MODE == 1) {
+                // The rings carry over into the stream's next row (whose bytes follow this row's); at the
+                // stream's end they drain: stage-B slot q holds the window ending at 128 - 2*kRing + q,
+                // stage-A slot q the one at 128 - kRing + q; stage-A survivors go to the queue with only
+                // their first probe known.
+                if ((uint32_t)r == R - 1) {
 #pragma unroll
-                // drain: stage-B slot q holds the window ending at 128 - 2*kRing + q, stage-A slot q the one at
-                // 128 - kRing + q; stage-A survivors go to the queue with only their first probe known
-                for (int q = 0; q < kRing; q++) {
-                    const bool pass2 = (__funnelshift_r(ring2_v[q], ring2_v[q], ring2_h[q]) & 1u) != 0;
-                    enqueue(pass2, (uint32_t)(kRowBytes - 2 * kRing + q), ring2_l[q], ring2_h[q], 2u);
-                    const bool pass1 = (__funnelshift_r(ring_v[q], ring_v[q], ring_l[q]) & 1u) != 0;
-                    enqueue(pass1, (uint32_t)(kRowBytes - kRing + q), ring_l[q], ring_h[q], 1u);
-                    ring_v[q] = 0;
-                    ring2_v[q] = 0;
+                    for (int q = 0; q < kRing; q++) {
+                        const bool pass2 = (__funnelshift_r(ring2_v[q], ring2_v[q], ring2_h[q]) & 1u) != 0;
+                        enqueue(pass2, (uint32_t)(2 * kRowBytes - 2 * kRing + q), ring2_l[q], ring2_h[q], 2u);
+                        const bool pass1 = (__funnelshift_r(ring_v[q], ring_v[q], ring_l[q]) & 1u) != 0;
+                        enqueue(pass1, (uint32_t)(2 * kRowBytes - kRing + q), ring_l[q], ring_h[q], 1u);
+                        ring_v[q] = 0;
+                        ring2_v[q] = 0;
+                    }
                 }
             }
             if (qn) {
