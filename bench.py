@@ -20,6 +20,7 @@ the text, filter loaded from a __bloom_filter_ cache; throughput = shard bytes /
 `processFile time` (the reference's own timer).
 """
 import argparse
+import collections
 import json
 import os
 import shutil
@@ -340,6 +341,10 @@ def run_batched(args, local):
     b = Batch(local)
     for f, w, o in zip(filters, jobs, offs):
         b.add(f, base + o, w.text_bytes)
+    # the autotuner picks each class of jobs' configuration; plain and batched forms both use it
+    t0 = time.perf_counter()
+    n_classes = b.autotune(16 << 20)
+    tune_s = time.perf_counter() - t0
     t0 = time.perf_counter()
     b.prepare()
     prepare_s = time.perf_counter() - t0
@@ -407,7 +412,10 @@ def run_batched(args, local):
         "ms_per_step": {"batched": t_batch * 1e3, "batched_device": statistics.median(dev_ms),
                         "plain_serial": t_plain * 1e3, "plain_streams": t_streams * 1e3},
         "bit_exact": {"plain_streams_vs_plain": same(got_streams, ref), "batched_vs_plain": same(got_batch, ref)},
-        "setup_s": {"generate_and_build": gen_s, "batch_prepare": prepare_s},
+        "setup_s": {"generate_and_build": gen_s, "autotune": tune_s, "batch_prepare": prepare_s},
+        "autotune_classes": n_classes,
+        "configs": dict(collections.Counter(f"{'dense' if f.config()[1] else 'sparse'}-{f.config()[0]}"
+                                            for f in filters)),
         "timing": "host clock between device-idle points, median of steps; batched_device = CUDA events",
     }
     b.close()

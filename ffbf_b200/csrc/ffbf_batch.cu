@@ -6,6 +6,7 @@
 #include <algorithm>
 #include <cstdio>
 #include <cstdlib>
+#include <map>
 #include <new>
 #include <string>
 #include <vector>
@@ -48,6 +49,9 @@ struct ffbf_batch {
     uint64_t graph_kernels = 0;  // kernel nodes of the graph
     cudaGraph_t graph = nullptr;
     cudaGraphExec_t exec = nullptr;
+    // branch streams and events used while capturing the graph's parallel branches
+    std::vector<cudaStream_t> branches;
+    std::vector<cudaEvent_t> events;
 };
 
 
@@ -111,20 +115,44 @@ ffbf_status build_plan(const std::vector<PlanJob>& jobs, int num_sms, ScanPlan& 
     return FFBF_OK;
 }
 
-cudaError_t launch_plan(const ScanPlan& p, const PlanDevice& d, int num_sms, cudaStream_t st) {
+cudaError_t launch_plan(const ScanPlan& p, const PlanDevice& d, int num_sms, cudaStream_t st,
+                        const cudaStream_t* branches, const cudaEvent_t* events) {
     cudaError_t e = ffbf::zero_counters(d.counters, d.n_counters, st);
-    for (size_t li = 0; li < p.launches.size() && e == cudaSuccess; li++) {
-        const PlanLaunch& L = p.launches[li];
-        e = ffbf::launch_fast_jobs(L.len, L.cfg, d.fast + L.off, L.n_jobs, L.n_items, L.max_s1, d.ctl + 4 * li, num_sms,
-                                   st);
+    const size_t nl = p.launches.size();
+    if (!branches) {
+        for (size_t li = 0; li < nl && e == cudaSuccess; li++) {
+            const PlanLaunch& L = p.launches[li];
+            e = ffbf::launch_fast_jobs(L.len, L.cfg, d.fast + L.off, L.n_jobs, L.n_items, L.max_s1, d.ctl + 4 * li,
+                                       num_sms, st);
+        }
+        if (e == cudaSuccess) e = ffbf::scan_generic_multi(d.args, d.tail, (uint32_t)p.tail.size(), num_sms, st);
+        return e;
     }
-    if (e == cudaSuccess) e = ffbf::scan_generic_multi(d.args, d.tail, (uint32_t)p.tail.size(), num_sms, st);
+    // fork: each tuned launch and the generic launch on its own branch (they touch disjoint tiles), join
+    // back on st; a branch's kernel takes SMs as the others' work queues drain
+    if (e == cudaSuccess) e = cudaEventRecord(events[0], st);
+    for (size_t li = 0; li <= nl && e == cudaSuccess; li++) {
+        cudaStream_t bs = branches[li];
+        e = cudaStreamWaitEvent(bs, events[0], 0);
+        if (e == cudaSuccess && li < nl) {
+            const PlanLaunch& L = p.launches[li];
+            e = ffbf::launch_fast_jobs(L.len, L.cfg, d.fast + L.off, L.n_jobs, L.n_items, L.max_s1, d.ctl + 4 * li,
+                                       num_sms, bs);
+        } else if (e == cudaSuccess) {
+            e = ffbf::scan_generic_multi(d.args, d.tail, (uint32_t)p.tail.size(), num_sms, bs);
+        }
+        if (e == cudaSuccess) e = cudaEventRecord(events[1 + li], bs);
+        if (e == cudaSuccess) e = cudaStreamWaitEvent(st, events[1 + li], 0);
+    }
     return e;
 }
 
 }  // namespace ffbf_host
 
 namespace {
+
+ffbf_status autotune_impl(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len, bool per_sm, int* threads,
+                          int* mode);
 
 ffbf_batch::Key batch_key(const ffbf_ctx* c) {
     return ffbf_batch::Key{c->d_main, c->d_ff,          c->d_hits,      c->d_counters, c->d_tiles,
@@ -140,6 +168,10 @@ ffbf_status bfail(ffbf_batch* b, ffbf_status s, const std::string& msg) {
 void batch_release(ffbf_batch* b) {
     if (b->exec) cudaGraphExecDestroy(b->exec);
     if (b->graph) cudaGraphDestroy(b->graph);
+    for (auto s : b->branches) cudaStreamDestroy(s);
+    for (auto e : b->events) cudaEventDestroy(e);
+    b->branches.clear();
+    b->events.clear();
     b->exec = nullptr;
     b->graph = nullptr;
     for (void* p : b->allocs) cudaFree(p);
@@ -245,8 +277,24 @@ ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
     // one graph: zero the jobs' counters, one tuned launch per group, one generic launch for all tail tiles
     if (cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal) != cudaSuccess)
         return bfail(b, FFBF_ECUDA, "stream capture failed to start");
+    for (size_t i = 0; i <= plan.launches.size(); i++) {
+        cudaStream_t bs;
+        if (cudaStreamCreateWithFlags(&bs, cudaStreamNonBlocking) != cudaSuccess) {
+            cudaGetLastError();
+            return bfail(b, FFBF_ECUDA, "branch stream creation failed");
+        }
+        b->branches.push_back(bs);
+    }
+    for (size_t i = 0; i <= plan.launches.size() + 1; i++) {
+        cudaEvent_t ev;
+        if (cudaEventCreateWithFlags(&ev, cudaEventDisableTiming) != cudaSuccess) {
+            cudaGetLastError();
+            return bfail(b, FFBF_ECUDA, "event creation failed");
+        }
+        b->events.push_back(ev);
+    }
     const uint64_t launches0 = ffbf::launches_total();
-    cudaError_t e = launch_plan(plan, d, b->num_sms, b->st);
+    cudaError_t e = launch_plan(plan, d, b->num_sms, b->st, b->branches.data(), b->events.data());
     cudaError_t e2 = cudaStreamEndCapture(b->st, &b->graph);
     b->graph_kernels = ffbf::launches_total() - launches0;  // counted again at each graph launch
     ffbf::unnote_launches(b->graph_kernels);
@@ -304,7 +352,58 @@ ffbf_status ffbf_batch_wait(ffbf_batch* b) {
     return FFBF_OK;
 }
 
-ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len, int* threads, int* mode) {
+ffbf_status ffbf_batch_autotune(ffbf_batch* b, size_t sample_bytes, uint32_t* n_classes) {
+    if (!b) return FFBF_EINVAL;
+    if (n_classes) *n_classes = 0;
+    // classes: jobs with the same geometry whose stage-1 tables are about as full (1/16 steps) scan alike
+    struct Class {
+        size_t rep;  // the class's largest job
+        std::vector<size_t> members;
+    };
+    std::map<std::vector<uint64_t>, Class> classes;
+    for (size_t i = 0; i < b->jobs.size(); i++) {
+        ffbf_ctx* c = b->jobs[i].c;
+        TRY(enter(c));
+        if (!use_fast(c, b->jobs[i].len)) continue;
+        TRY(prepare_fast(c));  // builds the stage-1 table and measures its fill
+        const std::vector<uint64_t> key = {c->g.len, c->g.k, c->g.s, c->g.cache_bits, c->g.nbits,
+                                           (uint64_t)(c->stage1_fill * 16.0)};
+        auto it = classes.find(key);
+        if (it == classes.end()) {
+            classes[key] = Class{i, {i}};
+        } else {
+            it->second.members.push_back(i);
+            if (b->jobs[i].len > b->jobs[it->second.rep].len) it->second.rep = i;
+        }
+    }
+    for (auto& kv : classes) {
+        const auto& rep = b->jobs[kv.second.rep];
+        size_t n = std::min(sample_bytes ? sample_bytes : (size_t)16 << 20, rep.len);
+        n = n / ffbf::kScanTile * ffbf::kScanTile;
+        if (n < ffbf::kScanTile) continue;
+        int threads = 0, mode = 0;
+        ffbf_status s = autotune_impl(rep.c, rep.text, n, true, &threads, &mode);
+        if (s != FFBF_OK) return bfail(b, s, std::string("autotune: ") + rep.c->err);
+        for (size_t m : kv.second.members) {
+            ffbf_ctx* c = b->jobs[m].c;
+            c->cfg = rep.c->cfg;
+            c->cfg_tuned = true;
+        }
+    }
+    if (n_classes) *n_classes = (uint32_t)classes.size();
+    batch_release(b);  // the next launch prepares with the tuned configurations
+    return FFBF_OK;
+}
+
+}  // extern "C"
+
+namespace {
+
+// Times the tuned scan's configurations on a sample and keeps the best. per_sm scores by SM-seconds per
+// byte (time x SMs the launch occupies): in a batch many jobs share the GPU, so a configuration whose
+// items fill fewer SMs on a small sample must not win by wall time alone. Otherwise by wall time.
+ffbf_status autotune_impl(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len, bool per_sm, int* threads,
+                          int* mode) {
     TRY(enter(c));
     if (!d_text || ((uintptr_t)d_text & 15)) return fail(c, FFBF_EINVAL, "device text must be 16-byte aligned");
     if (!use_fast(c, sample_len)) return fail(c, FFBF_EINVAL, "the tuned scan does not cover this geometry or size");
@@ -314,7 +413,7 @@ ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
     CUDA_TRY(c, cudaMemcpyAsync(saved, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
     const ffbf::FastConfig cands[] = {{512, 0, 0}, {384, 0, 0}, {256, 0, 0}, {384, 1, 0}, {256, 1, 0}};
     ffbf::FastConfig best = c->cfg;
-    float best_ms = 1e30f;
+    double best_score = 1e300;
     cudaEvent_t e0, e1;
     cudaEventCreate(&e0);
     cudaEventCreate(&e1);
@@ -336,8 +435,16 @@ ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
             if (rep > 0) ms = std::min(ms, t);  // the first run also builds the stage-1 table
         }
         if (s != FFBF_OK) break;
-        if (ms < best_ms) {
-            best_ms = ms;
+        double score = ms;
+        if (per_sm) {
+            const int t = ffbf::config_threads(cand);
+            const uint64_t bytes = sample_len / ffbf::kScanTile * ffbf::kScanTile;
+            const uint64_t streams = bytes / ((uint64_t)ffbf::fast_rows(sample_len, t, c->num_sms, false) * 128);
+            const uint64_t items = (streams + t - 1) / t;
+            score = ms * (double)std::min<uint64_t>(items, (uint64_t)c->num_sms);
+        }
+        if (score < best_score) {
+            best_score = score;
             best = cand;
         }
     }
@@ -356,6 +463,14 @@ ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
     if (threads) *threads = ffbf::config_threads(best);
     if (mode) *mode = best.mode;
     return s;
+}
+
+}  // namespace
+
+extern "C" {
+
+ffbf_status ffbf_autotune(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len, int* threads, int* mode) {
+    return autotune_impl(c, d_text, sample_len, false, threads, mode);
 }
 
 }  // extern "C"

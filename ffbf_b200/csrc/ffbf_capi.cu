@@ -876,6 +876,13 @@ ffbf_status ffbf_test_line(ffbf_ctx* c, const uint8_t* line, size_t len, int* hi
     return FFBF_OK;
 }
 
+ffbf_status ffbf_get_scan_config(const ffbf_ctx* c, int* threads, int* mode) {
+    if (!c) return FFBF_EINVAL;
+    if (threads) *threads = ffbf::config_threads(c->cfg);
+    if (mode) *mode = c->cfg.mode;
+    return FFBF_OK;
+}
+
 ffbf_status ffbf_clear_ff(ffbf_ctx* c) {
     TRY(enter(c));
     CUDA_TRY(c, cudaMemsetAsync(c->d_ff, 0, c->filter_bytes, c->st));

@@ -187,7 +187,9 @@ struct PlanDevice {
     uint32_t* ctl;        // 4 words per tuned launch: error flags, work-queue counter
 };
 // Enqueues a plan on st: zero every job's counters and control words, one tuned launch per group, one
-// generic launch over all tail tiles.
-cudaError_t launch_plan(const ScanPlan& p, const PlanDevice& d, int num_sms, cudaStream_t st);
+// generic launch over all tail tiles. With `branches` (launches + 1 streams) and `events` (launches + 2),
+// the launches run as parallel branches that fork from and join back to st.
+cudaError_t launch_plan(const ScanPlan& p, const PlanDevice& d, int num_sms, cudaStream_t st,
+                        const cudaStream_t* branches = nullptr, const cudaEvent_t* events = nullptr);
 
 }  // namespace ffbf_host

@@ -191,6 +191,10 @@ ffbf_status ffbf_batch_wait(ffbf_batch* b);
 void* ffbf_batch_stream(ffbf_batch* b);
 const char* ffbf_batch_last_error(const ffbf_batch* b);
 void ffbf_batch_destroy(ffbf_batch* b);
+/* Autotunes a batch's jobs by class: jobs with the same geometry and a similar stage-1 table fill form a
+ * class; ffbf_autotune times the configurations on the first `sample_bytes` (0: 16 MiB) of the class's
+ * largest text, and every job of the class takes the winner. The next launch prepares again. */
+ffbf_status ffbf_batch_autotune(ffbf_batch* b, size_t sample_bytes, uint32_t* n_classes);
 
 /* Scan server: pattern sets resident on the device, scan requests admitted while device memory allows,
  * and every admitted request whose text has reached the device scanned together in the next launch
@@ -244,6 +248,11 @@ void ffbf_server_destroy(ffbf_server* s);  /* waits for work on the device; unfi
  * of the context, and reports it (threads, mode: 0 shared-memory stage, 1 pipelined L2 probes). The
  * feed-forward filter is left unchanged. Without it, the placement follows the stage-1 table's fill. */
 ffbf_status ffbf_autotune(ffbf_ctx* ctx, const uint8_t* d_text, size_t sample_len, int* threads, int* mode);
+
+/* The tuned scan's current configuration for this context (CTA threads; mode 0 shared-memory stage 1,
+ * 1 pipelined L2 probes), as the autotuner or the filter's fill chose it. Before the first scan or tuning
+ * it reports the defaults. */
+ffbf_status ffbf_get_scan_config(const ffbf_ctx* ctx, int* threads, int* mode);
 
 /* Zeroes the feed-forward filter (a fresh reverseBitvector, ffbf.cpp:107). Enqueued on the context's
  * stream; later calls on the context see it done. */
