@@ -432,6 +432,12 @@ void ffbf_destroy(ffbf_ctx* c) {
     c->allocs.clear();
     if (c->h_counters) cudaFreeHost(c->h_counters);
     if (c->h_job) cudaFreeHost(c->h_job);
+    if (c->h_jobs) cudaFreeHost(c->h_jobs);
+    for (auto ev : c->pipe_events) cudaEventDestroy(ev);
+    if (c->st_copy) {
+        cudaStreamSynchronize(c->st_copy);
+        cudaStreamDestroy(c->st_copy);
+    }
     if (c->st) cudaStreamDestroy(c->st);
     cudaGetLastError();
     delete c;
@@ -673,6 +679,91 @@ ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
     return FFBF_OK;
 }
 
+}  // extern "C"
+
+namespace {
+
+constexpr uint64_t kPipeChunk = 128ull << 20;  // bytes per overlapped copy of a host text
+
+// The scan of a host text whose copy to the device overlaps the scan: the text goes over in chunks of
+// about kPipeChunk bytes on the context's copy stream, and after each chunk the tuned kernel runs over
+// the work items whose bytes (and halos) have landed. Every chunk's launch uses the whole text's tensor
+// map and absolute positions; its descriptor only shifts the item numbering (item_begin = -first item).
+ffbf_status scan_host_pipelined(ffbf_ctx* c, const uint8_t* text, size_t len) {
+    TRY(setup_scan_state(c, c->d_text_own, len));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * sizeof(uint32_t), c->st));
+    TRY(prepare_fast(c));
+    c->scan_path = 1;
+    const ffbf::ScanArgs a = make_scan_args(c);
+    const int threads = ffbf::config_threads(c->cfg);
+    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(len, threads, c->num_sms, false);
+    ffbf::FastJob job;
+    cudaError_t e;
+    const uint64_t covered = ffbf::fill_fast_job(a, c->d_stage1, c->cfg, rows, &job, &e);
+    if (e != cudaSuccess) return fail(c, FFBF_ECUDA, "tensor map encoding failed");
+    const uint64_t item_bytes = (uint64_t)threads * rows * 128;
+    const uint32_t per_chunk = (uint32_t)std::max<uint64_t>(1, kPipeChunk / item_bytes);
+    const uint32_t n_chunks = (job.n_supertiles + per_chunk - 1) / per_chunk;
+    if (!c->st_copy) CUDA_TRY(c, cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
+    while (c->pipe_events.size() < (size_t)n_chunks + 2) {
+        cudaEvent_t ev;
+        CUDA_TRY(c, cudaEventCreateWithFlags(&ev, cudaEventDisableTiming));
+        c->pipe_events.push_back(ev);
+    }
+    if (c->jobs_cap < n_chunks) {
+        TRY(sync(c));  // the old staging may still feed a copy
+        if (c->h_jobs) cudaFreeHost(c->h_jobs);
+        c->h_jobs = nullptr;
+        dfree(c, c->d_jobs);
+        c->jobs_cap = 0;
+        if (cudaMallocHost(&c->h_jobs, n_chunks * sizeof(ffbf::FastJob)) != cudaSuccess) {
+            cudaGetLastError();
+            c->h_jobs = nullptr;
+            return fail(c, FFBF_ENOMEM_HOST, "pinned chunk descriptors");
+        }
+        TRY(dalloc_t(c, &c->d_jobs, n_chunks));
+        c->jobs_cap = n_chunks;
+    }
+    TRY(sync(c));  // the staging array is rewritten below; earlier uploads must be done
+    for (uint32_t i = 0; i < n_chunks; i++) {
+        c->h_jobs[i] = job;
+        c->h_jobs[i].item_begin = 0u - i * per_chunk;  // item k of chunk i is supertile i * per_chunk + k
+    }
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_jobs, c->h_jobs, n_chunks * sizeof(ffbf::FastJob), cudaMemcpyHostToDevice,
+                                c->st));
+    // the copies overwrite the text buffer: start them after what the context's stream already holds
+    CUDA_TRY(c, cudaEventRecord(c->pipe_events[n_chunks + 1], c->st));
+    CUDA_TRY(c, cudaStreamWaitEvent(c->st_copy, c->pipe_events[n_chunks + 1], 0));
+    uint64_t copied = 0;
+    for (uint32_t i = 0; i < n_chunks; i++) {
+        const uint32_t first = i * per_chunk;
+        const uint32_t count = std::min(per_chunk, job.n_supertiles - first);
+        const uint64_t end = std::min<uint64_t>(len, (uint64_t)(first + count) * item_bytes);
+        if (end > copied) {
+            CUDA_TRY(c, cudaMemcpyAsync(c->d_text_own + copied, text + copied, end - copied, cudaMemcpyHostToDevice,
+                                        c->st_copy));
+            copied = end;
+        }
+        CUDA_TRY(c, cudaEventRecord(c->pipe_events[i], c->st_copy));
+        CUDA_TRY(c, cudaStreamWaitEvent(c->st, c->pipe_events[i], 0));
+        CUDA_TRY(c, cudaMemsetAsync(c->d_counters + ffbf::CNT_QUEUE, 0, sizeof(uint32_t), c->st));
+        CUDA_TRY(c, ffbf::launch_fast_jobs(c->g.len, c->cfg, c->d_jobs + i, 1, count, job.stage1_nwords,
+                                           c->d_counters + ffbf::CNT_ERROR, c->num_sms, c->st));
+    }
+    if (copied < len) {
+        CUDA_TRY(c, cudaMemcpyAsync(c->d_text_own + copied, text + copied, len - copied, cudaMemcpyHostToDevice,
+                                    c->st_copy));
+    }
+    CUDA_TRY(c, cudaEventRecord(c->pipe_events[n_chunks], c->st_copy));
+    CUDA_TRY(c, cudaStreamWaitEvent(c->st, c->pipe_events[n_chunks], 0));
+    CUDA_TRY(c, ffbf::scan_tail(a, covered, c->st));
+    return FFBF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 ffbf_status ffbf_scan(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_result* out) {
     TRY(enter(c));
     if (!text && len) return fail(c, FFBF_EINVAL, "text is NULL");
@@ -681,6 +772,11 @@ ffbf_status ffbf_scan(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_re
         c->text_cap = 0;
         TRY(dalloc_t(c, &c->d_text_own, len + 64));
         c->text_cap = len + 64;
+    }
+    if (len >= 2 * kPipeChunk && use_fast(c, len)) {
+        TRY(scan_host_pipelined(c, text, len));
+        c->scan_pending = true;
+        return ffbf_scan_collect(c, out);
     }
     if (len) CUDA_TRY(c, cudaMemcpyAsync(c->d_text_own, text, len, cudaMemcpyHostToDevice, c->st));
     TRY(ffbf_scan_device(c, c->d_text_own, len));

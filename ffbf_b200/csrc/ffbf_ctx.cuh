@@ -64,6 +64,12 @@ struct ffbf_ctx {
     // A context whose filters (main, feed-forward, stage-1 table) belong to another context: a served
     // request's scan state attached to a resident pattern set. It never frees or rebuilds them.
     bool borrowed = false;
+    // host-text scans with the copy overlapped: a copy stream, one event per chunk, per-chunk descriptors
+    cudaStream_t st_copy = nullptr;
+    std::vector<cudaEvent_t> pipe_events;
+    ffbf::FastJob* h_jobs = nullptr;  // pinned
+    ffbf::FastJob* d_jobs = nullptr;
+    uint32_t jobs_cap = 0;
     ffbf::FastJob* h_job = nullptr;  // pinned staging of a plain scan's job descriptor
     ffbf::FastJob* d_job = nullptr;
     std::vector<uint64_t> r_hits, r_ls, r_le;

@@ -229,3 +229,29 @@ def test_line_resolution_over_many_tile_blocks():
         np.testing.assert_array_equal(r.line_start, s["line_start"])
         np.testing.assert_array_equal(r.line_end, s["line_end"])
         np.testing.assert_array_equal(f.get_filters()[1], o.ff)
+
+
+def test_host_text_scan_with_overlapped_copy_equals_oracle():
+    """A host text of at least two 128 MiB chunks is copied in chunks while the scan runs on the chunks that
+    have landed; windows, lines and the feed-forward filter equal the oracle's, including windows and a
+    50 MiB line across chunk boundaries."""
+    from ffbf_b200 import datagen as dg
+
+    prm = Params(20, 5, 2, 1 << 24, 1 << 28)
+    pats = dg.gen_patterns(41, dg.PRINTABLE, 3000, 20, 40)
+    text = dg.gen_text(42, dg.PRINTABLE, 300 << 20, 2000)
+    seg = text[(100 << 20) - 1000:(150 << 20)]
+    seg[seg == 10] = ord("y")
+    dg.plant(43, pats, text, 4000)
+    for k in range(1, 3):  # occurrences straddling the first chunk boundaries
+        text[(k << 27) - 10:(k << 27) - 10 + 25] = np.frombuffer(pats[:25].tobytes(), dtype=np.uint8)
+    o = oracle.Oracle.from_params(prm)
+    o.build(pats)
+    s = o.scan(text)
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        r = f.process(text)
+        np.testing.assert_array_equal(r.hit_offsets, s["hits"])
+        np.testing.assert_array_equal(r.line_start, s["line_start"])
+        np.testing.assert_array_equal(r.line_end, s["line_end"])
+        np.testing.assert_array_equal(f.get_filters()[1], o.ff)
