@@ -972,6 +972,33 @@ ffbf_status ffbf_test_line(ffbf_ctx* c, const uint8_t* line, size_t len, int* hi
     return FFBF_OK;
 }
 
+ffbf_status ffbf_debug_scan_unpublished(ffbf_ctx* c, const uint8_t* d_text, size_t len, uint32_t spins) {
+    TRY(enter(c));
+    if (!use_fast(c, len)) return fail(c, FFBF_EINVAL, "the tuned scan does not cover this geometry or size");
+    TRY(setup_scan_state(c, d_text, len));
+    if (!c->d_gate) TRY(dalloc_t(c, &c->d_gate, 1));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_gate, 0, sizeof(uint32_t), c->st));  // never published
+    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * sizeof(uint32_t), c->st));
+    TRY(prepare_fast(c));
+    const ffbf::ScanArgs a = make_scan_args(c);
+    const int threads = ffbf::config_threads(c->cfg);
+    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(len, threads, c->num_sms, false);
+    cudaError_t e;
+    ffbf::fill_fast_job(a, c->d_stage1, c->cfg, rows, c->h_job, &e);
+    if (e != cudaSuccess) return fail(c, FFBF_ECUDA, "tensor map encoding failed");
+    c->h_job->ready = c->d_gate;
+    c->h_job->ready_spins = spins;
+    CUDA_TRY(c, cudaMemcpyAsync(c->d_job, c->h_job, sizeof(ffbf::FastJob), cudaMemcpyHostToDevice, c->st));
+    CUDA_TRY(c, ffbf::launch_fast_jobs(c->g.len, c->cfg, c->d_job, 1, c->h_job->n_supertiles, c->h_job->stage1_nwords,
+                                       c->d_counters + ffbf::CNT_ERROR, c->num_sms, c->st));
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_counters, c->d_counters, ffbf::CNT_WORDS * 4, cudaMemcpyDeviceToHost, c->st));
+    TRY(sync(c));
+    reset_scan(c);
+    if (c->h_counters[ffbf::CNT_ERROR] & 4u)
+        return fail(c, FFBF_ETIMEOUT, "the scan's publication gate stayed closed for %u polls", spins);
+    return fail(c, FFBF_ESTATE, "the unpublished scan did not time out");
+}
+
 ffbf_status ffbf_get_scan_config(const ffbf_ctx* c, int* threads, int* mode) {
     if (!c) return FFBF_EINVAL;
     if (threads) *threads = ffbf::config_threads(c->cfg);

@@ -71,6 +71,7 @@ struct ffbf_ctx {
     ffbf::FastJob* d_jobs = nullptr;
     uint32_t jobs_cap = 0;
     ffbf::FastJob* h_job = nullptr;  // pinned staging of a plain scan's job descriptor
+    uint32_t* d_gate = nullptr;      // a publication word that stays zero (ffbf_debug_scan_unpublished)
     ffbf::FastJob* d_job = nullptr;
     std::vector<uint64_t> r_hits, r_ls, r_le;
 

@@ -273,7 +273,22 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
         mbar_init(bar0, 1);
         mbar_init(bar1, 1);
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
-        issue(0);
+        // publication gate: a bounded poll, and no load in flight if it gives up
+        bool open = true;
+        if (const uint32_t* rw = jobs[0].ready) {
+            const uint32_t spins = jobs[0].ready_spins;
+            for (uint32_t i = 0;; i++) {
+                if (*reinterpret_cast<const volatile uint32_t*>(rw) != 0u) break;
+                if (i >= spins) {
+                    atomicOr(error_flag, 4u);
+                    open = false;
+                    break;
+                }
+                __nanosleep(1000);
+            }
+        }
+        if (open) issue(0);
+        else meta[3] = 0;
     }
     __syncthreads();
 

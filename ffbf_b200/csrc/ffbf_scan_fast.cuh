@@ -23,11 +23,14 @@ struct alignas(64) FastJob {
     uint32_t stage1_shift;         // the table holds C >> shift bits (0: exact copy of the cache region)
     HitRec* hits;
     uint32_t hits_cap;
-    uint32_t pad;
+    uint32_t ready_spins;  // polls of *ready before the launch gives up (about 1 us each)
     uint32_t* counters;
     long long* tile_first_nl;
     long long* tile_last_nl;
     uint64_t n_tiles;  // 16 KiB tiles of the text (bounds the newline summary writes)
+    // Optional publication gate of the launch (read from its first job): no load is issued until *ready is
+    // non-zero; a gate still closed after ready_spins polls ends the launch with the timeout flag.
+    const uint32_t* ready;
 };
 
 // How a job is scanned: CTA size (256/384/512), probe mode (0: sparse, shared-memory stage 1; 1: dense,

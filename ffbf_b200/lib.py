@@ -37,7 +37,7 @@ EXPORTED = [
     "ffbf_test_line", "ffbf_clear_ff", "ffbf_get_filters", "ffbf_filter_bytes", "ffbf_free", "ffbf_format_spans",
     "ffbf_stream", "ffbf_kernel_launches", "ffbf_scan_static", "ffbf_batch_create", "ffbf_batch_add",
     "ffbf_batch_prepare", "ffbf_batch_launch", "ffbf_batch_wait", "ffbf_batch_stream", "ffbf_batch_last_error",
-    "ffbf_batch_destroy", "ffbf_batch_autotune", "ffbf_autotune", "ffbf_get_scan_config", "ffbf_server_create", "ffbf_server_add_set", "ffbf_server_submit",
+    "ffbf_batch_destroy", "ffbf_batch_autotune", "ffbf_autotune", "ffbf_get_scan_config", "ffbf_debug_scan_unpublished", "ffbf_server_create", "ffbf_server_add_set", "ffbf_server_submit",
     "ffbf_server_poll", "ffbf_server_release", "ffbf_server_get_stats", "ffbf_server_last_error",
     "ffbf_server_destroy",
 ]
@@ -152,6 +152,7 @@ def load_library(path=LIB_PATH):
         "ffbf_batch_destroy": (None, [vp]),
         "ffbf_batch_autotune": (ctypes.c_int, [vp, sz, P(ctypes.c_uint32)]),
         "ffbf_get_scan_config": (ctypes.c_int, [vp, P(ctypes.c_int), P(ctypes.c_int)]),
+        "ffbf_debug_scan_unpublished": (ctypes.c_int, [vp, vp, sz, ctypes.c_uint32]),
         "ffbf_autotune": (ctypes.c_int, [vp, vp, sz, P(ctypes.c_int), P(ctypes.c_int)]),
         "ffbf_server_create": (ctypes.c_int, [ctypes.c_int, ctypes.c_uint64, ctypes.c_uint32, P(vp)]),
         "ffbf_server_add_set": (ctypes.c_int, [vp, vp, P(ctypes.c_uint32)]),
@@ -357,6 +358,11 @@ class Filter:
         t, m = ctypes.c_int(), ctypes.c_int()
         self._check(self._lib.ffbf_autotune(self._h, ctypes.c_void_p(dev_ptr), n, ctypes.byref(t), ctypes.byref(m)))
         return t.value, m.value
+
+    def debug_scan_unpublished(self, dev_ptr, n, spins=2000):
+        """Failure-detection check: a scan gated on a word that is never published; raises FFBFError with
+        FFBF_ETIMEOUT (4) after `spins` polls of about a microsecond."""
+        self._check(self._lib.ffbf_debug_scan_unpublished(self._h, ctypes.c_void_p(dev_ptr), n, spins))
 
     def config(self):
         """(threads, mode) of the tuned scan for this filter (mode 0: shared-memory stage, 1: L2 probes)."""

@@ -249,6 +249,12 @@ void ffbf_server_destroy(ffbf_server* s);  /* waits for work on the device; unfi
  * feed-forward filter is left unchanged. Without it, the placement follows the stage-1 table's fill. */
 ffbf_status ffbf_autotune(ffbf_ctx* ctx, const uint8_t* d_text, size_t sample_len, int* threads, int* mode);
 
+/* Failure-detection check (no counterpart in the reference, which has no device waits): runs the tuned
+ * scan of d_text gated on a device word that is never published. The kernel polls the word `spins` times
+ * (about a microsecond apart), records the timeout and ends before issuing any load; the call returns
+ * FFBF_ETIMEOUT and the context stays usable. Nothing is scanned and no result is kept. */
+ffbf_status ffbf_debug_scan_unpublished(ffbf_ctx* ctx, const uint8_t* d_text, size_t len, uint32_t spins);
+
 /* The tuned scan's current configuration for this context (CTA threads; mode 0 shared-memory stage 1,
  * 1 pipelined L2 probes), as the autotuner or the filter's fill chose it. Before the first scan or tuning
  * it reports the defaults. */
