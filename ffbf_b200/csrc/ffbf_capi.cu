@@ -265,6 +265,11 @@ ffbf_status setup_scan_state(ffbf_ctx* c, const uint8_t* d_text, size_t len) {
     if (!d_text && len) return fail(c, FFBF_EINVAL, "text pointer is NULL");
     if (((uintptr_t)d_text & 15) != 0) return fail(c, FFBF_EINVAL, "device text must be 16-byte aligned");
     reset_scan(c);
+    if (!c->keep_records) {  // a scan of one device text ends any segmented scan's state
+        c->segmented = false;
+        c->segs.clear();
+        c->seg_hr.clear();
+    }
     const uint64_t ntiles = (len + ffbf::kScanTile - 1) / ffbf::kScanTile;
     if (c->tiles_cap < ntiles) {
         dfree(c, c->d_tiles);
@@ -664,6 +669,8 @@ ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
             CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->d_hitlines, nh * sizeof(HitLine), cudaMemcpyDeviceToHost, c->st));
         }
         TRY(sync(c));
+        if (c->keep_records)  // a segment of a larger text: ffbf_verify needs its records again
+            for (uint32_t i = 0; i < nh; i++) c->seg_hr.push_back(HitRec{hr[i].off + c->seg_base, hr[i].h});
         order_hits(hr.data(), hl.data(), nh, c->r_hits, c->r_ls, c->r_le);
         c->scan_pending = false;
         c->have_scan = true;
@@ -764,9 +771,12 @@ ffbf_status scan_host_pipelined(ffbf_ctx* c, const uint8_t* text, size_t len) {
 
 extern "C" {
 
-ffbf_status ffbf_scan(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_result* out) {
-    TRY(enter(c));
-    if (!text && len) return fail(c, FFBF_EINVAL, "text is NULL");
+}  // extern "C"
+
+namespace {
+
+// One host text that fits the device: copied (overlapped with the scan when large) and scanned.
+ffbf_status scan_one(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_result* out) {
     if (c->text_cap < len + 64) {
         dfree(c, c->d_text_own);
         c->text_cap = 0;
@@ -781,6 +791,103 @@ ffbf_status ffbf_scan(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_re
     if (len) CUDA_TRY(c, cudaMemcpyAsync(c->d_text_own, text, len, cudaMemcpyHostToDevice, c->st));
     TRY(ffbf_scan_device(c, c->d_text_own, len));
     return ffbf_scan_collect(c, out);
+}
+
+// Device bytes a scan of `len` text bytes needs beyond what the context holds: the text buffer, the tile
+// summaries and, the first time, the hit buffers.
+uint64_t scan_need(const ffbf_ctx* c, uint64_t len) {
+    const uint64_t ntiles = (len + ffbf::kScanTile - 1) / ffbf::kScanTile;
+    uint64_t need = len + 64 + 8 * (4 * ntiles + 2 * ffbf::tile_agg_words(ntiles));
+    if (!c->d_hits) need += 2 * kInitialHitsCap * 16;
+    return need;
+}
+
+// The largest segment a scan may put on the device: what the HBM budget (or the device's free memory, less
+// 1 GiB) leaves after everything but the text buffer, three quarters of it; 0 when the whole text fits.
+ffbf_status segment_size(ffbf_ctx* c, uint64_t len, uint64_t* seg) {
+    *seg = 0;
+    uint64_t avail;
+    if (c->budget) {
+        avail = c->budget > c->used ? c->budget - c->used : 0;
+    } else {
+        size_t fr = 0, tot = 0;
+        CUDA_TRY(c, cudaMemGetInfo(&fr, &tot));
+        avail = fr > (1ull << 30) ? fr - (1ull << 30) : 0;
+    }
+    avail += c->text_cap;  // the current text buffer is given back first
+    if (scan_need(c, len) <= avail) return FFBF_OK;
+    *seg = avail / 4 * 3 / 65536 * 65536;
+    if (*seg < (1u << 20)) return fail(c, FFBF_ENOMEM_DEVICE, "no room on the device for a 1 MiB text segment");
+    return FFBF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+ffbf_status ffbf_scan(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_result* out) {
+    TRY(enter(c));
+    if (!text && len) return fail(c, FFBF_EINVAL, "text is NULL");
+    c->segmented = false;
+    c->keep_records = false;
+    c->segs.clear();
+    c->seg_hr.clear();
+    uint64_t seg = 0;
+    TRY(segment_size(c, len, &seg));
+    if (seg == 0) return scan_one(c, text, len, out);
+    // A text larger than the device holds: scan it in segments that end just after a '\n'. A valid window
+    // never spans a '\n', so the segments' scans are independent; their results are offset and joined, and
+    // the feed-forward filter accumulates over them as over successive scans.
+    dfree(c, c->d_text_own);
+    c->text_cap = 0;
+    std::vector<uint64_t> hits, ls, le;
+    c->keep_records = true;
+    for (uint64_t pos = 0; pos < len;) {
+        uint64_t end = std::min<uint64_t>(len, pos + seg);
+        if (end < len) {
+            const void* nl = memrchr(text + pos, '\n', end - pos);
+            if (!nl) {
+                c->keep_records = false;
+                return fail(c, FFBF_EINVAL, "a line longer than the device's text segment (%llu bytes) at offset %llu",
+                            (unsigned long long)seg, (unsigned long long)pos);
+            }
+            end = (uint64_t)((const uint8_t*)nl - text) + 1;
+        }
+        c->seg_base = pos;
+        c->segs.push_back({pos, end - pos, (uint64_t)c->seg_hr.size(), 0});
+        ffbf_scan_result r{};
+        ffbf_status st = scan_one(c, text + pos, end - pos, &r);
+        if (st != FFBF_OK) {
+            c->keep_records = false;
+            return st;
+        }
+        c->segs.back().hr_end = c->seg_hr.size();
+        for (uint64_t i = 0; i < r.n_hits; i++) hits.push_back(r.hit_offsets[i] + pos);
+        for (uint64_t i = 0; i < r.n_lines; i++) {
+            ls.push_back(r.line_start[i] + pos);
+            le.push_back(r.line_end[i] + pos);
+        }
+        pos = end;
+    }
+    c->keep_records = false;
+    c->segmented = true;
+    c->seg_text = text;
+    c->r_hits.swap(hits);
+    c->r_ls.swap(ls);
+    c->r_le.swap(le);
+    c->nhits = (uint32_t)c->r_hits.size();
+    c->text_len = len;
+    c->have_scan = true;
+    c->scan_pending = false;
+    if (out) {
+        out->text_len = len;
+        out->n_hits = c->r_hits.size();
+        out->hit_offsets = c->r_hits.data();
+        out->n_lines = c->r_ls.size();
+        out->line_start = c->r_ls.data();
+        out->line_end = c->r_le.data();
+    }
+    return FFBF_OK;
 }
 
 ffbf_status ffbf_format_lines(ffbf_ctx* c, const uint8_t* text, size_t len, size_t chunk, uint8_t** out,
@@ -882,6 +989,57 @@ ffbf_status ffbf_format_pruned(ffbf_ctx* c, size_t chunk, uint8_t** out, size_t*
     return s;
 }
 
+}  // extern "C"
+
+namespace {
+
+// Verifies nh hit records already in c->d_hits against a device text, appending (offset + base, pattern)
+// pairs. The match buffers grow and the pass reruns when they overflow.
+ffbf_status verify_pass(ffbf_ctx* c, uint32_t nh, const uint8_t* d_text, uint64_t text_len, uint64_t tsize,
+                        uint64_t base, std::vector<uint64_t>& off_out, std::vector<uint32_t>& pid_out) {
+    if (c->match_cap < std::max<uint32_t>(1024, nh)) {
+        dfree(c, c->d_moff);
+        dfree(c, c->d_mpid);
+        c->match_cap = 0;
+        uint32_t cap = std::max<uint32_t>(1024, nh);
+        TRY(dalloc_t(c, &c->d_moff, cap));
+        TRY(dalloc_t(c, &c->d_mpid, cap));
+        c->match_cap = cap;
+    }
+    for (int attempt = 0; attempt < 2; attempt++) {
+        CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * 4, c->st));
+        CUDA_TRY(c, ffbf::verify_hits(c->d_hits, nh, d_text, text_len, c->d_keys, c->d_vals, tsize - 1, c->d_pat,
+                                      c->d_pstart, c->d_pend, c->d_moff, c->d_mpid, c->match_cap, c->d_counters, c->st));
+        CUDA_TRY(c, cudaMemcpyAsync(c->h_counters, c->d_counters, ffbf::CNT_WORDS * 4, cudaMemcpyDeviceToHost, c->st));
+        TRY(sync(c));
+        uint32_t nm = c->h_counters[ffbf::CNT_MATCHES];
+        if (nm <= c->match_cap) break;
+        uint64_t cap = (uint64_t)nm + nm / 4 + 1024;
+        if (cap > 0xffffffffull) return fail(c, FFBF_EINVAL, "more than 2^32 matches");
+        dfree(c, c->d_moff);
+        dfree(c, c->d_mpid);
+        c->match_cap = 0;
+        TRY(dalloc_t(c, &c->d_moff, cap));
+        TRY(dalloc_t(c, &c->d_mpid, cap));
+        c->match_cap = (uint32_t)cap;
+    }
+    const uint32_t nm = c->h_counters[ffbf::CNT_MATCHES];
+    const size_t at = off_out.size();
+    off_out.resize(at + nm);
+    pid_out.resize(at + nm);
+    if (nm) {
+        CUDA_TRY(c, cudaMemcpyAsync(off_out.data() + at, c->d_moff, nm * 8ull, cudaMemcpyDeviceToHost, c->st));
+        CUDA_TRY(c, cudaMemcpyAsync(pid_out.data() + at, c->d_mpid, nm * 4ull, cudaMemcpyDeviceToHost, c->st));
+    }
+    TRY(sync(c));
+    for (size_t i = at; i < off_out.size(); i++) off_out[i] += base;
+    return FFBF_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
 ffbf_status ffbf_verify(ffbf_ctx* c, ffbf_matches* out) {
     TRY(enter(c));
     if (c->scan_pending) TRY(ffbf_scan_collect(c, nullptr));
@@ -897,44 +1055,43 @@ ffbf_status ffbf_verify(ffbf_ctx* c, ffbf_matches* out) {
         TRY(dalloc_t(c, &c->d_vals, tsize));
         c->table_cap = tsize;
     }
-    const uint32_t nh = c->nhits;
-    if (c->match_cap < std::max<uint32_t>(1024, nh)) {
-        dfree(c, c->d_moff);
-        dfree(c, c->d_mpid);
-        c->match_cap = 0;
-        uint32_t cap = std::max<uint32_t>(1024, nh);
-        TRY(dalloc_t(c, &c->d_moff, cap));
-        TRY(dalloc_t(c, &c->d_mpid, cap));
-        c->match_cap = cap;
-    }
-    for (int attempt = 0; attempt < 2; attempt++) {
-        CUDA_TRY(c, cudaMemsetAsync(c->d_vals, 0xff, tsize * 4, c->st));
-        CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * 4, c->st));
-        CUDA_TRY(c, ffbf::table_build(c->d_ids, c->nids, c->d_phash, c->d_keys, c->d_vals, tsize - 1, c->d_counters, c->st));
-        CUDA_TRY(c, ffbf::verify_hits(c->d_hits, nh, c->d_text, c->text_len, c->d_keys, c->d_vals, tsize - 1, c->d_pat,
-                                      c->d_pstart, c->d_pend, c->d_moff, c->d_mpid, c->match_cap, c->d_counters, c->st));
-        CUDA_TRY(c, cudaMemcpyAsync(c->h_counters, c->d_counters, ffbf::CNT_WORDS * 4, cudaMemcpyDeviceToHost, c->st));
-        TRY(sync(c));
-        if (c->h_counters[ffbf::CNT_ERROR]) return fail(c, FFBF_ECUDA, "verification table overflow");
-        uint32_t nm = c->h_counters[ffbf::CNT_MATCHES];
-        if (nm <= c->match_cap) break;
-        uint64_t cap = (uint64_t)nm + nm / 4 + 1024;
-        if (cap > 0xffffffffull) return fail(c, FFBF_EINVAL, "more than 2^32 matches");
-        dfree(c, c->d_moff);
-        dfree(c, c->d_mpid);
-        c->match_cap = 0;
-        TRY(dalloc_t(c, &c->d_moff, cap));
-        TRY(dalloc_t(c, &c->d_mpid, cap));
-        c->match_cap = (uint32_t)cap;
-    }
-    const uint32_t nm = c->h_counters[ffbf::CNT_MATCHES];
-    std::vector<uint64_t> off(nm);
-    std::vector<uint32_t> pid(nm);
-    if (nm) {
-        CUDA_TRY(c, cudaMemcpyAsync(off.data(), c->d_moff, nm * 8ull, cudaMemcpyDeviceToHost, c->st));
-        CUDA_TRY(c, cudaMemcpyAsync(pid.data(), c->d_mpid, nm * 4ull, cudaMemcpyDeviceToHost, c->st));
-    }
+    CUDA_TRY(c, cudaMemsetAsync(c->d_vals, 0xff, tsize * 4, c->st));
+    CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * 4, c->st));
+    CUDA_TRY(c, ffbf::table_build(c->d_ids, c->nids, c->d_phash, c->d_keys, c->d_vals, tsize - 1, c->d_counters, c->st));
+    CUDA_TRY(c, cudaMemcpyAsync(c->h_counters, c->d_counters, ffbf::CNT_WORDS * 4, cudaMemcpyDeviceToHost, c->st));
     TRY(sync(c));
+    if (c->h_counters[ffbf::CNT_ERROR]) return fail(c, FFBF_ECUDA, "verification table overflow");
+    std::vector<uint64_t> off;
+    std::vector<uint32_t> pid;
+    if (!c->segmented) {
+        TRY(verify_pass(c, c->nhits, c->d_text, c->text_len, tsize, 0, off, pid));
+    } else {
+        // the text was scanned in segments: each segment's text goes back to the device with its hit records
+        for (const auto& sg : c->segs) {
+            const uint64_t nh = sg.hr_end - sg.hr_begin;
+            if (!nh) continue;
+            if (c->hits_cap < nh) {
+                dfree(c, c->d_hits);
+                dfree(c, c->d_hitlines);
+                c->hits_cap = 0;
+                TRY(dalloc_t(c, &c->d_hits, nh));
+                TRY(dalloc_t(c, &c->d_hitlines, nh));
+                c->hits_cap = (uint32_t)nh;
+            }
+            if (c->text_cap < sg.len + 64) {
+                dfree(c, c->d_text_own);
+                c->text_cap = 0;
+                TRY(dalloc_t(c, &c->d_text_own, sg.len + 64));
+                c->text_cap = sg.len + 64;
+            }
+            std::vector<HitRec> rel(c->seg_hr.begin() + sg.hr_begin, c->seg_hr.begin() + sg.hr_end);
+            for (auto& h : rel) h.off -= sg.pos;
+            CUDA_TRY(c, cudaMemcpyAsync(c->d_text_own, c->seg_text + sg.pos, sg.len, cudaMemcpyHostToDevice, c->st));
+            CUDA_TRY(c, cudaMemcpyAsync(c->d_hits, rel.data(), nh * sizeof(HitRec), cudaMemcpyHostToDevice, c->st));
+            TRY(verify_pass(c, (uint32_t)nh, c->d_text_own, sg.len, tsize, sg.pos, off, pid));
+        }
+    }
+    const size_t nm = off.size();
     std::vector<uint32_t> order(nm);
     for (uint32_t i = 0; i < nm; i++) order[i] = i;
     std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {

@@ -72,6 +72,16 @@ struct ffbf_ctx {
     uint32_t jobs_cap = 0;
     ffbf::FastJob* h_job = nullptr;  // pinned staging of a plain scan's job descriptor
     uint32_t* d_gate = nullptr;      // a publication word that stays zero (ffbf_debug_scan_unpublished)
+    // a host text scanned in line-aligned segments (larger than the device holds): the text, the segments
+    // and every hit record (absolute offsets, in segment order), which ffbf_verify uses segment by segment
+    struct Segment {
+        uint64_t pos, len, hr_begin, hr_end;
+    };
+    bool segmented = false, keep_records = false;
+    const uint8_t* seg_text = nullptr;
+    uint64_t seg_base = 0;
+    std::vector<Segment> segs;
+    std::vector<ffbf::HitRec> seg_hr;
     ffbf::FastJob* d_job = nullptr;
     std::vector<uint64_t> r_hits, r_ls, r_le;
 

@@ -113,7 +113,11 @@ typedef struct {
 /* processFile (ffbf.cpp:310-392) over a host text image: the hash rolls over every line ('\n' resets it
  * and is not hashed); every window whose K main bits are set marks its line and sets K bits of the
  * feed-forward filter in getHashValue_2 order (ffbf.cpp:161-185). The feed-forward filter accumulates
- * over successive scans, as it does over one reference run; ffbf_clear_ff starts a new one. */
+ * over successive scans, as it does over one reference run; ffbf_clear_ff starts a new one.
+ * A text of 256 MiB or more is copied in chunks while the chunks already on the device are scanned. A text
+ * larger than the device can hold (its free memory, or the context's HBM budget) is scanned in segments
+ * that each end after a '\n' (a line longer than a segment gives FFBF_EINVAL); the results are the same,
+ * and ffbf_verify then copies the segments again, so the text must stay valid until ffbf_verify. */
 ffbf_status ffbf_scan(ffbf_ctx* ctx, const uint8_t* text, size_t len, ffbf_scan_result* out);
 
 /* The same scan over a text already in device memory (16-byte aligned), enqueued on the context's

@@ -255,3 +255,34 @@ def test_host_text_scan_with_overlapped_copy_equals_oracle():
         np.testing.assert_array_equal(r.line_start, s["line_start"])
         np.testing.assert_array_equal(r.line_end, s["line_end"])
         np.testing.assert_array_equal(f.get_filters()[1], o.ff)
+
+
+def test_text_larger_than_the_device_budget_is_scanned_in_segments():
+    """A host text that does not fit the context's HBM budget is scanned in line-aligned segments; hits,
+    lines, the feed-forward filter, the prune and the verified matches equal the oracle's, and stdout
+    formatting over the whole text is unchanged."""
+    from ffbf_b200 import datagen as dg
+
+    prm = Params(20, 5, 2, 1 << 20, 1 << 24)
+    pats = dg.gen_patterns(51, dg.PRINTABLE, 3000, 20, 40)
+    text = dg.gen_text(52, dg.PRINTABLE, 40 << 20, 200)
+    dg.plant(53, pats, text, 3000)
+    o, s, pr, ooff, opid = run_oracle(prm, pats, text)
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        f.set_hbm_budget(32 << 20)  # about 24 MB left beside the filters: segments of about 18 MB
+        r = f.process(text)
+        np.testing.assert_array_equal(r.hit_offsets, s["hits"])
+        np.testing.assert_array_equal(r.line_start, s["line_start"])
+        np.testing.assert_array_equal(r.line_end, s["line_end"])
+        assert f.format_lines(text) == s["out"]
+        np.testing.assert_array_equal(f.get_filters()[1], o.ff)
+        np.testing.assert_array_equal(f.filter_phrases(), pr["ids"])
+        off, pid = f.verify()
+        np.testing.assert_array_equal(off, ooff)
+        np.testing.assert_array_equal(pid, opid)
+        # a line longer than a segment cannot be split
+        one_line = np.full(30 << 20, ord("a"), dtype=np.uint8)
+        with pytest.raises(FFBFError) as e:
+            f.process(one_line)
+        assert e.value.status == 1
