@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                   f"-I{os.path.join(ROOT, 'include')}"]
 
-CUDA_SOURCES = ["ffbf_kernels.cu", "ffbf_scan_fast.cu", "ffbf_capi.cu", "ffbf_batch.cu", "ffbf_serve.cu", "ffbf_static.cu"]
+CUDA_SOURCES = ["ffbf_kernels.cu", "ffbf_scan_fast.cu", "ffbf_capi.cu", "ffbf_batch.cu", "ffbf_serve.cu", "ffbf_static.cu", "ffbf_hashbench.cu"]
 
 
 def _newer(target, deps):
@@ -72,6 +72,12 @@ def build(force=False, verbose=False):
         _run(["g++", "-std=c++17", "-O2", "-Wall", f"-I{os.path.join(ROOT, 'include')}", cli_src, "-o", cli + ".tmp",
               f"-L{OUT}", "-lffbf", "-Wl,-rpath,$ORIGIN"])
         os.replace(cli + ".tmp", cli)
+    hb_src = os.path.join(CSRC, "hashbench_cli.cpp")
+    hb = os.path.join(OUT, "hashbench")
+    if os.path.exists(hb_src) and (force or _newer(hb, [hb_src, lib] + hdrs)):
+        _run(["g++", "-std=c++17", "-O2", "-Wall", f"-I{os.path.join(ROOT, 'include')}", hb_src, "-o", hb + ".tmp",
+              f"-L{OUT}", "-lffbf", "-Wl,-rpath,$ORIGIN"])
+        os.replace(hb + ".tmp", hb)
     gen_src = os.path.join(CSRC, "datagen.c")
     gen = os.path.join(OUT, "libffbf_datagen.so")
     if force or _newer(gen, [gen_src]):

@@ -305,6 +305,22 @@ ffbf_status ffbf_scan_static(const ffbf_params* p, const uint32_t* d_main, uint3
                              uint64_t len, uint64_t* d_hit_offsets, uint64_t* d_line_start, uint64_t* d_line_end,
                              uint32_t* n_hits, void* stream);
 
+/* The reference's hash benchmark (src/hashes/hashbench.cc:60-130) for the scan's hash,
+ * hash_rot_sbox_pre_2<19>, with the hashing on `device`. Raw bytes are hashed (hashbench does not map bytes
+ * >= 0x80 to 0 as the filter does).
+ *
+ * ffbf_hashbench_lines is `hashbench -l` (hash_lines, :108-127): for every piece fgets(buf, 4095, f) would
+ * return (a line through its '\n', or the next 4094 bytes of a longer line) the hash restarts, the bytes up
+ * to the first NUL or '\n' are hashed, and "%x %s\n" prints hval() (the hash's high 32 bits) and that
+ * string. *out holds exactly the bytes the reference prints; release it with ffbf_free.
+ *
+ * ffbf_hashbench_file is `hashbench -f` (hash_file, :60-99): the hash rolls over every byte with no restart.
+ * The reference prints only the byte count and the time; here *xor_of_hashes is the XOR of the 64-bit hash
+ * after every byte (a checkable result) and *seconds the device time of that pass (copy excluded). */
+ffbf_status ffbf_hashbench_lines(int device, const uint8_t* text, size_t len, uint8_t** out, size_t* out_len);
+ffbf_status ffbf_hashbench_file(int device, const uint8_t* text, size_t len, uint64_t* xor_of_hashes,
+                                double* seconds);
+
 /* Releases memory the library allocated for an out-parameter. */
 void ffbf_free(void* p);
 

@@ -75,6 +75,10 @@ def _load():
         lib.orc_load_filter.argtypes = [P(OParams), vp, sz, vp]
         lib.orc_verify.restype = ctypes.c_int
         lib.orc_verify.argtypes = [P(OParams), vp, sz, vp, sz, vp, sz, vp, sz, P(_Matches)]
+        lib.orc_hashbench_lines.restype = ctypes.c_long
+        lib.orc_hashbench_lines.argtypes = [vp, sz, P(vp)]
+        lib.orc_hash_xor.restype = ctypes.c_uint64
+        lib.orc_hash_xor.argtypes = [vp, sz, ctypes.c_int]
         lib.orc_free.restype = None
         lib.orc_free.argtypes = [vp]
         _lib = lib
@@ -248,3 +252,20 @@ def decode_filter_file(data):
     """Set-bit indices stored in a __bloom_filter_ image (cumulative uint32 deltas)."""
     d = np.frombuffer(data[: len(data) // 4 * 4], dtype="<u4").astype(np.uint64)
     return (np.cumsum(d) & 0xFFFFFFFF).astype(np.uint64)
+
+
+def hashbench_lines(text):
+    """What `hashbench -l` prints for `text` (hash_rot_sbox_pre_2<19>, hashbench.cc:108-127)."""
+    lib = _load()
+    t = _np(text)
+    out = ctypes.c_void_p()
+    n = lib.orc_hashbench_lines(_p(t), t.size, ctypes.byref(out))
+    if n < 0:
+        raise MemoryError("oracle hashbench failed")
+    return _take(lib, out.value, n, np.uint8).tobytes()
+
+
+def hash_xor(text, length=19):
+    """XOR of the rolling hash after every byte of `text` (no resets): the checkable result of hashbench -f."""
+    t = _np(text)
+    return int(_load().orc_hash_xor(_p(t), t.size, length))

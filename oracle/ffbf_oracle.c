@@ -18,6 +18,7 @@
 #include <string.h>
 
 #include "../ffbf_b200/csrc/ffbf_sbox.h"
+#include <stdio.h>
 
 static const uint64_t ORC_SBOX[256] = {FFBF_SBOX_WORDS};
 
@@ -381,6 +382,62 @@ int orc_verify(const orc_params* p, const uint8_t* pats, size_t plen, const uint
     free(head); free(next); free(st.p); free(en.p);
     m->off = off.p; m->pid = pid.p; m->n = off.n;
     return 0;
+}
+
+/* ---- hashbench (src/hashes/hashbench.cc), HashTester<hash_rot_sbox_pre_2<19>, 19> -------------- */
+
+/* hash_rot_sbox_pre_2::update (:42-51) on the raw byte: hashbench does not map bytes >= 0x80. */
+static inline void hash_update_raw(orc_hash* x, uint8_t c) {
+    x->h = rol64(x->h, 1);
+    x->h ^= ORC_SBOX[c];
+    x->h ^= x->b[x->bufptr];
+    x->b[x->bufptr++] = rol64(ORC_SBOX[c], x->len);
+    if (x->bufptr >= x->len) { x->bufptr = 0; x->full = 1; }
+}
+
+/* hash_lines (hashbench.cc:108-127): fgets(buf, 4095, f) returns a line with its '\n', or the next 4094
+ * bytes of a longer line; per piece the hash is reset, every byte up to the first NUL is hashed except the
+ * '\n' (which becomes the string's end), and "%x %s\n" prints hval() = h >> 32 and the string.
+ * Writes the printed bytes to *out (malloc'd) and returns their count, or -1 on allocation failure. */
+long orc_hashbench_lines(const uint8_t* text, size_t n, uint8_t** out) {
+    size_t cap = n * 2 + 64, o = 0;
+    uint8_t* buf = (uint8_t*)malloc(cap);
+    if (!buf) return -1;
+    for (size_t pos = 0; pos < n;) {
+        size_t m = 0; /* fgets: up to 4094 bytes, through the first '\n' */
+        while (m < 4094 && pos + m < n) {
+            m++;
+            if (text[pos + m - 1] == '\n') break;
+        }
+        orc_hash x; x.len = 19; hash_reset(&x);
+        size_t e = 0; /* the C string: up to the first NUL or '\n' */
+        while (e < m && text[pos + e] != 0 && text[pos + e] != '\n') hash_update_raw(&x, text[pos + e++]);
+        if (o + e + 16 > cap) {
+            cap = (o + e + 16) * 2;
+            uint8_t* nb = (uint8_t*)realloc(buf, cap);
+            if (!nb) { free(buf); return -1; }
+            buf = nb;
+        }
+        o += (size_t)sprintf((char*)buf + o, "%x ", (uint32_t)(x.h >> 32));
+        memcpy(buf + o, text + pos, e);
+        o += e;
+        buf[o++] = '\n';
+        pos += m;
+    }
+    *out = buf;
+    return (long)o;
+}
+
+/* hash_file (hashbench.cc:60-99) hashes every byte with no reset and prints only the byte count and the
+ * time; as a checkable result, the XOR of the 64-bit hash after every byte. */
+uint64_t orc_hash_xor(const uint8_t* text, size_t n, int len) {
+    orc_hash x; x.len = len; hash_reset(&x);
+    uint64_t acc = 0;
+    for (size_t i = 0; i < n; i++) {
+        hash_update_raw(&x, text[i]);
+        acc ^= x.h;
+    }
+    return acc;
 }
 
 void orc_free(void* ptr) { free(ptr); }

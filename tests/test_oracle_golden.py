@@ -91,3 +91,46 @@ def test_fixtures_are_current(name):
     r = oracle.run_reference(oracle.ref_binary(prm), pats, text=text.tobytes())
     assert g.matches("stdout", r["stdout"]) and g.matches("bloom", r["bloom"])
     assert g.matches("pruned", r["pruned"]) and g.matches("index", r["index"])
+
+
+def test_hashbench_restatement_matches_reference_output():
+    """oracle.hashbench_lines reproduces `hashbench -l` (the reference's own binary, tests/golden/hashbench)
+    byte for byte: fgets pieces of at most 4094 bytes, hashing stopped at a NUL, raw bytes >= 0x80."""
+    import gzip
+    import os
+
+    import oracle
+
+    d = os.path.join(os.path.dirname(__file__), "golden", "hashbench")
+    text = gzip.open(os.path.join(d, "input.bin.gz")).read()
+    want = gzip.open(os.path.join(d, "lines.out.gz")).read()
+    assert oracle.hashbench_lines(text) == want
+
+
+def test_hash_xor_restatement_is_the_rolling_hash():
+    """oracle.hash_xor follows hash_rot_sbox_pre_2::update byte by byte (checked against the window closed
+    form on random bytes)."""
+    import numpy as np
+
+    import oracle
+
+    import os
+    import re
+
+    hdr = open(os.path.join(os.path.dirname(os.path.dirname(__file__)), "ffbf_b200", "csrc", "ffbf_sbox.h")).read()
+    sbox = [int(w, 16) for w in re.findall(r"0x([0-9a-fA-F]+)ull", hdr)]
+    assert len(sbox) == 256
+    rng = np.random.default_rng(5)
+    t = rng.integers(0, 256, 3000, dtype=np.uint8)
+
+    def rol(w, s):
+        s %= 64
+        return ((w << s) | (w >> (64 - s))) & 0xFFFFFFFFFFFFFFFF if s else w
+
+    acc = 0
+    for i in range(t.size):
+        h = 0
+        for j in range(max(0, i - 18), i + 1):
+            h ^= rol(int(sbox[t[j]]), i - j)
+        acc ^= h
+    assert oracle.hash_xor(t) == acc
