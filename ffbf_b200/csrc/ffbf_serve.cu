@@ -120,8 +120,14 @@ struct ffbf_server {
 
 namespace {
 
-ffbf_status sfail(ffbf_server* s, ffbf_status st, const std::string& msg) {
+// The last error is written by the caller's thread and by the worker; both go through the mutex.
+void set_err(ffbf_server* s, const std::string& msg) {
+    std::lock_guard<std::mutex> lk(s->mu);
     s->err = msg;
+}
+
+ffbf_status sfail(ffbf_server* s, ffbf_status st, const std::string& msg) {
+    set_err(s, msg);
     return st;
 }
 
@@ -227,7 +233,7 @@ void launch_ready(ffbf_server* s) {
     if (st == FFBF_OK && plan.launches.size() + 1 > kMaxCtl) st = FFBF_EINVAL;
     if (st == FFBF_OK && !ensure_tail(s, plan.tail.size() + 1)) st = FFBF_ENOMEM_DEVICE;
     if (st != FFBF_OK) {
-        if (st != FFBF_EINVAL && bad < jobs.size()) s->err = jobs[bad].c->err;
+        if (st != FFBF_EINVAL && bad < jobs.size()) set_err(s, jobs[bad].c->err);
         for (Request* r : batch) finish(s, r, st);
         return;
     }
@@ -257,7 +263,7 @@ void launch_ready(ffbf_server* s) {
     if (e == cudaSuccess) e = cudaEventRecord(s->batch_done, s->st_scan);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        s->err = std::string("batch launch failed: ") + cudaGetErrorString(e);
+        set_err(s, std::string("batch launch failed: ") + cudaGetErrorString(e));
         for (Request* r : batch) finish(s, r, FFBF_ECUDA);
         return;
     }
@@ -282,7 +288,7 @@ void collect_slow(ffbf_server* s) {
         r->ls.assign(res.line_start, res.line_start + res.n_lines);
         r->le.assign(res.line_end, res.line_end + res.n_lines);
     } else {
-        s->err = slot->err;
+        set_err(s, slot->err);
     }
     finish(s, r, st);
 }
@@ -318,7 +324,7 @@ ffbf_status start_resolve(ffbf_server* s, Request* r) {
     if (e == cudaSuccess) e = cudaEventRecord(h.done, c->st);
     if (e != cudaSuccess) {
         cudaGetLastError();
-        s->err = std::string("result copy failed: ") + cudaGetErrorString(e);
+        set_err(s, std::string("result copy failed: ") + cudaGetErrorString(e));
         return FFBF_ECUDA;
     }
     return FFBF_OK;
@@ -553,10 +559,12 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
 ffbf_status ffbf_server_add_set(ffbf_server* s, ffbf_ctx* set, uint32_t* set_id) {
     if (!s || !set || !set_id) return FFBF_EINVAL;
     if (set->device != s->device) return sfail(s, FFBF_EINVAL, "the set's context is on another device");
+    bool started;
     {
         std::lock_guard<std::mutex> lk(s->mu);
-        if (s->started) return sfail(s, FFBF_ESTATE, "sets are registered before the first submit");
+        started = s->started;
     }
+    if (started) return sfail(s, FFBF_ESTATE, "sets are registered before the first submit");
     ffbf_status st = enter(set);
     if (st == FFBF_OK && ffbf::fast_scan_supported(set->g, ffbf::kScanTile) && !set->force_generic) st = prepare_fast(set);
     if (st == FFBF_OK) st = sync(set);
@@ -635,7 +643,14 @@ ffbf_status ffbf_server_get_stats(ffbf_server* s, ffbf_server_stats* out) {
     return FFBF_OK;
 }
 
-const char* ffbf_server_last_error(const ffbf_server* s) { return s ? s->err.c_str() : "null server"; }
+const char* ffbf_server_last_error(const ffbf_server* s) {
+    if (!s) return "null server";
+    // a copy per calling thread: the worker may set a new message meanwhile
+    static thread_local std::string copy;
+    std::lock_guard<std::mutex> lk(const_cast<ffbf_server*>(s)->mu);
+    copy = s->err;
+    return copy.c_str();
+}
 
 void ffbf_server_destroy(ffbf_server* s) {
     if (!s) return;
