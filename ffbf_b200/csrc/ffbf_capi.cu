@@ -454,6 +454,19 @@ uint64_t ffbf_filter_bytes(const ffbf_ctx* c) { return c ? c->filter_bytes : 0; 
 
 void ffbf_free(void* p) { free(p); }
 
+void* ffbf_host_alloc(size_t bytes) {
+    void* p = nullptr;
+    if (cudaMallocHost(&p, bytes ? bytes : 1) != cudaSuccess) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    return p;
+}
+
+void ffbf_host_free(void* p) {
+    if (p) cudaFreeHost(p);
+}
+
 void* ffbf_stream(ffbf_ctx* c) { return c ? (void*)c->st : nullptr; }
 
 uint64_t ffbf_kernel_launches(void) { return ffbf::launches_total(); }

@@ -45,6 +45,40 @@ bool read_fd(int fd, std::vector<uint8_t>& out) {
     }
 }
 
+// A text buffer: page-locked (from the library) when stdin is a regular file of known size, so that the scan's
+// copy to the device runs at full speed and overlaps the scan; a growing vector otherwise (pipes).
+struct TextBuf {
+    uint8_t* pinned = nullptr;
+    size_t n = 0;
+    std::vector<uint8_t> vec;
+    const uint8_t* data() const { return pinned ? pinned : vec.data(); }
+    size_t size() const { return pinned ? n : vec.size(); }
+    ~TextBuf() {
+        if (pinned) ffbf_host_free(pinned);
+    }
+};
+
+bool read_stdin(TextBuf& t) {
+    struct stat st;
+    if (fstat(0, &st) == 0 && S_ISREG(st.st_mode) && st.st_size > 0) {
+        const off_t here = lseek(0, 0, SEEK_CUR);
+        const size_t want = (size_t)(st.st_size - (here > 0 ? here : 0));
+        t.pinned = (uint8_t*)ffbf_host_alloc(want ? want : 1);
+        if (t.pinned) {
+            size_t got = 0;
+            while (got < want) {
+                ssize_t r = read(0, t.pinned + got, want - got);
+                if (r < 0) return false;
+                if (r == 0) break;
+                got += (size_t)r;
+            }
+            t.n = got;
+            return true;
+        }
+    }
+    return read_fd(0, t.vec);
+}
+
 bool read_file(const char* path, std::vector<uint8_t>& out) {
     FILE* f = fopen(path, "rb");
     if (!f) return false;
@@ -138,9 +172,9 @@ int main(int argc, char** argv) {
         return -1;
     }
 
-    std::vector<uint8_t> text;
+    TextBuf text;
     double t0 = now();
-    if (!read_fd(0, text)) {
+    if (!read_stdin(text)) {
         perror("Error");
         return die(c, FFBF_EIO, "Error while reading from file");
     }

@@ -321,6 +321,12 @@ ffbf_status ffbf_hashbench_lines(int device, const uint8_t* text, size_t len, ui
 ffbf_status ffbf_hashbench_file(int device, const uint8_t* text, size_t len, uint64_t* xor_of_hashes,
                                 double* seconds);
 
+/* Page-locked host memory (cudaMallocHost) for texts that ffbf_scan copies to the device: copies from it run
+ * at full PCIe speed and overlap the scan, where pageable memory is staged. NULL on failure; release it with
+ * ffbf_host_free. No counterpart in the reference. */
+void* ffbf_host_alloc(size_t bytes);
+void ffbf_host_free(void* p);
+
 /* Releases memory the library allocated for an out-parameter. */
 void ffbf_free(void* p);
 
