@@ -239,6 +239,7 @@ ffbf_status ffbf_batch_add(ffbf_batch* b, ffbf_ctx* c, const uint8_t* d_text, si
 }
 
 ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
+    NvtxRange nvtx_("ffbf_batch_prepare");
     if (!b) return FFBF_EINVAL;
     if (cudaSetDevice(b->device) != cudaSuccess) return bfail(b, FFBF_ECUDA, "cudaSetDevice failed");
     batch_release(b);
@@ -308,6 +309,7 @@ ffbf_status ffbf_batch_prepare(ffbf_batch* b) {
 }
 
 ffbf_status ffbf_batch_launch(ffbf_batch* b) {
+    NvtxRange nvtx_("ffbf_batch_launch");
     if (!b) return FFBF_EINVAL;
     bool stale = !b->prepared || b->keys.size() != b->jobs.size();
     for (size_t i = 0; i < b->jobs.size() && !stale; i++)
@@ -353,6 +355,7 @@ ffbf_status ffbf_batch_wait(ffbf_batch* b) {
 }
 
 ffbf_status ffbf_batch_autotune(ffbf_batch* b, size_t sample_bytes, uint32_t* n_classes) {
+    NvtxRange nvtx_("ffbf_batch_autotune");
     if (!b) return FFBF_EINVAL;
     if (n_classes) *n_classes = 0;
     // classes: jobs with the same geometry whose stage-1 tables are about as full (1/16 steps) scan alike

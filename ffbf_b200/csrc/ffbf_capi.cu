@@ -529,6 +529,7 @@ ffbf_status ffbf_set_patterns(ffbf_ctx* c, const uint8_t* file, size_t len) {
 }
 
 ffbf_status ffbf_build(ffbf_ctx* c) {
+    NvtxRange nvtx_("ffbf_build");
     TRY(enter(c));
     if (!c->have_patterns) return fail(c, FFBF_ESTATE, "ffbf_build needs ffbf_set_patterns first");
     CUDA_TRY(c, ffbf::hash_patterns(c->d_pat, c->d_pstart, c->d_pend, c->npat, c->g, c->d_phash, c->d_main, 1, c->st));
@@ -639,6 +640,7 @@ ffbf_status ffbf_save_filter_file(ffbf_ctx* c, const char* path) {
 }
 
 ffbf_status ffbf_scan_device(ffbf_ctx* c, const uint8_t* d_text, size_t len) {
+    NvtxRange nvtx_("ffbf_scan_device");
     TRY(enter(c));
     TRY(setup_scan_state(c, d_text, len));
     TRY(launch_scan(c));
@@ -647,6 +649,7 @@ ffbf_status ffbf_scan_device(ffbf_ctx* c, const uint8_t* d_text, size_t len) {
 }
 
 ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
+    NvtxRange nvtx_("ffbf_scan_collect");
     TRY(enter(c));
     if (!c->scan_pending && !c->have_scan) return fail(c, FFBF_ESTATE, "no scan to collect");
     if (c->scan_pending) {
@@ -839,6 +842,7 @@ ffbf_status segment_size(ffbf_ctx* c, uint64_t len, uint64_t* seg) {
 extern "C" {
 
 ffbf_status ffbf_scan(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_result* out) {
+    NvtxRange nvtx_("ffbf_scan");
     TRY(enter(c));
     if (!text && len) return fail(c, FFBF_EINVAL, "text is NULL");
     c->segmented = false;
@@ -933,6 +937,7 @@ ffbf_status ffbf_format_spans(const uint8_t* buf, size_t len, const uint64_t* st
 }
 
 ffbf_status ffbf_prune(ffbf_ctx* c, ffbf_prune_result* out) {
+    NvtxRange nvtx_("ffbf_prune");
     TRY(enter(c));
     if (!c->have_patterns) return fail(c, FFBF_ESTATE, "ffbf_prune needs ffbf_set_patterns first");
     if (c->scan_pending) TRY(ffbf_scan_collect(c, nullptr));
@@ -1054,6 +1059,7 @@ ffbf_status verify_pass(ffbf_ctx* c, uint32_t nh, const uint8_t* d_text, uint64_
 extern "C" {
 
 ffbf_status ffbf_verify(ffbf_ctx* c, ffbf_matches* out) {
+    NvtxRange nvtx_("ffbf_verify");
     TRY(enter(c));
     if (c->scan_pending) TRY(ffbf_scan_collect(c, nullptr));
     if (!c->have_scan) return fail(c, FFBF_ESTATE, "ffbf_verify needs a scan first");

@@ -9,9 +9,19 @@
 #include <string>
 #include <vector>
 
+#include <nvtx3/nvToolsExt.h>
+
 #include "../../include/ffbf.h"
 #include "ffbf_kernels.cuh"
 #include "ffbf_scan_fast.cuh"
+
+// A named NVTX range over a C-ABI call, for profilers (`ncu --nvtx`): the phases of the path show by name.
+struct NvtxRange {
+    explicit NvtxRange(const char* name) { nvtxRangePushA(name); }
+    ~NvtxRange() { nvtxRangePop(); }
+    NvtxRange(const NvtxRange&) = delete;
+    NvtxRange& operator=(const NvtxRange&) = delete;
+};
 
 struct ffbf_ctx {
     ffbf_params prm{};

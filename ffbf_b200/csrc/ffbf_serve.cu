@@ -218,6 +218,7 @@ bool ensure_tail(ffbf_server* s, size_t n) {
 
 // Launches every ready request as one plan on the scan stream.
 void launch_ready(ffbf_server* s) {
+    NvtxRange nvtx_("server batch launch");
     std::vector<PlanJob> jobs;
     std::vector<Request*> batch;
     for (Request* r : s->ready) {

@@ -144,6 +144,19 @@ public:
 
     ffbf_ctx* handle() { return ctx_; }
 
+    // The context with every queued pattern built into its filter, for the batch and server wrappers below.
+    ffbf_ctx* built_handle() {
+        flush();
+        return ctx_;
+    }
+
+    // The results of the last scan of this filter's context (a batch job's, once the batch is waited for).
+    ffbf_scan_result collect() {
+        ffbf_scan_result r;
+        check(ffbf_scan_collect(ctx_, &r));
+        return r;
+    }
+
 private:
     void check(ffbf_status s) {
         if (s != FFBF_OK) throw FilterError(std::string(ffbf_status_string(s)) + ": " + ffbf_last_error(ctx_));
@@ -159,6 +172,73 @@ private:
     ffbf_ctx* ctx_ = nullptr;
     std::vector<uint8_t> pending_;
     bool dirty_ = false;
+};
+
+// Many (filter, device text) jobs scanned in one graph launch (ffbf_batch_* in ffbf.h). The reference has no
+// counterpart; each job's results come from its filter's collect() after wait().
+class Batch {
+public:
+    explicit Batch(int device = 0) {
+        ffbf_status s = ffbf_batch_create(device, &b_);
+        if (s != FFBF_OK) throw FilterError(std::string("Not able to create a batch: ") + ffbf_status_string(s));
+    }
+    ~Batch() { ffbf_batch_destroy(b_); }
+    Batch(const Batch&) = delete;
+    Batch& operator=(const Batch&) = delete;
+
+    void add(Filter& f, const uint8_t* d_text, size_t len) { check(ffbf_batch_add(b_, f.built_handle(), d_text, len)); }
+    uint32_t autotune(size_t sample_bytes = 0) {
+        uint32_t n = 0;
+        check(ffbf_batch_autotune(b_, sample_bytes, &n));
+        return n;
+    }
+    void launch() { check(ffbf_batch_launch(b_)); }
+    void wait() { check(ffbf_batch_wait(b_)); }
+
+private:
+    void check(ffbf_status s) {
+        if (s != FFBF_OK) throw FilterError(std::string(ffbf_status_string(s)) + ": " + ffbf_batch_last_error(b_));
+    }
+    ffbf_batch* b_ = nullptr;
+};
+
+// Resident pattern sets and a request loop with continuous batching (ffbf_server_* in ffbf.h). No counterpart
+// in the reference. Register the filters before the first submit; a result's arrays stay valid until
+// release(request_id).
+class Server {
+public:
+    explicit Server(int device = 0, uint64_t arena_bytes = 0, uint32_t slots = 0) {
+        ffbf_status s = ffbf_server_create(device, arena_bytes, slots, &s_);
+        if (s != FFBF_OK) throw FilterError(std::string("Not able to create a server: ") + ffbf_status_string(s));
+    }
+    ~Server() { ffbf_server_destroy(s_); }
+    Server(const Server&) = delete;
+    Server& operator=(const Server&) = delete;
+
+    uint32_t add_set(Filter& f) {
+        uint32_t id = 0;
+        check(ffbf_server_add_set(s_, f.built_handle(), &id));
+        return id;
+    }
+    uint64_t submit(uint32_t set, const uint8_t* text, size_t len) {
+        uint64_t id = 0;
+        check(ffbf_server_submit(s_, set, text, len, &id));
+        return id;
+    }
+    std::vector<ffbf_request_result> poll(uint32_t max = 64, uint32_t wait_us = 0) {
+        std::vector<ffbf_request_result> out(max);
+        uint32_t n = 0;
+        check(ffbf_server_poll(s_, out.data(), max, &n, wait_us));
+        out.resize(n);
+        return out;
+    }
+    void release(uint64_t request_id) { check(ffbf_server_release(s_, request_id)); }
+
+private:
+    void check(ffbf_status s) {
+        if (s != FFBF_OK) throw FilterError(std::string(ffbf_status_string(s)) + ": " + ffbf_server_last_error(s_));
+    }
+    ffbf_server* s_ = nullptr;
 };
 
 }  // namespace ffbf

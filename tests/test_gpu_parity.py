@@ -5,6 +5,7 @@ offsets, line spans, feed-forward bit array; prune -> pruned file + __index_ fil
 (offset, pattern id) pairs. All comparisons are bit-exact.
 """
 import os
+import re
 import subprocess
 import tempfile
 
@@ -286,3 +287,26 @@ def test_text_larger_than_the_device_budget_is_scanned_in_segments():
         with pytest.raises(FFBFError) as e:
             f.process(one_line)
         assert e.value.status == 1
+
+
+def test_cpp_mirror_program_matches_reference_files(tmp_path):
+    """A C++ program driving ffbf::Filter like the reference's main prints the reference's stdout and writes its
+    pruned and index files (golden plain_small); its server request finds the direct scan's hits."""
+    from test_host_cpu import build_mirror_example
+
+    exe = build_mirror_example(str(tmp_path))
+    g = Golden("plain_small")
+    prm, pats, text = build_inputs("plain_small")
+    (tmp_path / "pats").write_bytes(pats)
+    (tmp_path / "text").write_bytes(text.tobytes())
+    for mode in ([], ["server"]):
+        with open(tmp_path / "text", "rb") as fin:
+            r = subprocess.run([exe, "20", "pats", "out"] + mode, stdin=fin, capture_output=True, cwd=tmp_path)
+        assert r.returncode == 0, r.stderr
+        assert g.matches("stdout", r.stdout)
+        assert g.matches("pruned", (tmp_path / "out").read_bytes())
+        assert g.matches("index", (tmp_path / "__index_out").read_bytes())
+        direct = int(re.search(rb"direct scan: (\d+) hits", r.stderr).group(1))
+        if mode:
+            served = int(re.search(rb"status 0, (\d+) hits", r.stderr).group(1))
+            assert served == direct > 0

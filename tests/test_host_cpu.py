@@ -94,3 +94,24 @@ def test_cli_usage_error():
     r = subprocess.run([cli, "only_one_arg"], capture_output=True)
     assert r.returncode == 255
     assert b"Usage: ffbf phrases phrases.out < corpus > filtered_corpus" in r.stderr
+
+
+def build_mirror_example(out_dir):
+    """Compiles tests/cpp/mirror_example.cpp against include/ffbf.hpp and links it to libffbf.so."""
+    exe = os.path.join(out_dir, "mirror_example")
+    lib = os.path.join(ROOT, "ffbf_b200", "_lib")
+    subprocess.run(["g++", "-std=c++17", "-O2", "-Wall", "-Werror", f"-I{os.path.join(ROOT, 'include')}",
+                    os.path.join(ROOT, "tests", "cpp", "mirror_example.cpp"), "-o", exe, f"-L{lib}", "-lffbf",
+                    f"-Wl,-rpath,{lib}"], check=True, capture_output=True)
+    return exe
+
+
+def test_cpp_mirror_header_compiles_and_links(tmp_path):
+    """include/ffbf.hpp (Filter, Batch, Server) compiles warning-free in a program written like the reference's
+    main and links against the library; without a device the program reports FilterError, not a crash."""
+    exe = build_mirror_example(str(tmp_path))
+    if has_gpu():
+        return
+    (tmp_path / "pats").write_bytes(b"abcdefghijklmnopqrstuvwxyz\n")
+    r = subprocess.run([exe, "20", "pats", "out"], input=b"text\n", capture_output=True, cwd=tmp_path)
+    assert r.returncode == 1 and b"FilterError" in r.stderr
