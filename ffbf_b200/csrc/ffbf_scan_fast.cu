@@ -298,7 +298,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
 
     // the current job's parameters (reloaded when the job changes)
     int cur_job = -1;
-    uint32_t R = 0, cmask = 0, s1_bmask = 0, p2_mask = 0, p2_add = 0, s1_first = 0, spt_log2 = 0;
+    uint32_t R = 0, cmask = 0, s1_bmask = 0, p2_mask = 0, p2_add = 0, s1_first = 0, spt_log2 = 0, one_probe = 0;
     bool two = false;
     auto job_desc = [&]() { return jobs + cur_job; };
     // The filter pointer is held in a register: the loop's global stores would otherwise make the compiler
@@ -374,6 +374,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             s1_fits = MODE != 0 || J->stage1_nwords <= max_s1_words;
             cmask = g.cache_mask;
             two = g.s > 1;
+            one_probe = two ? 0u : 1u;
             // stage-1 table of T = C >> shift bits, folded modulo T: the byte offset of bit (h & (T-1))'s
             // word is (h >> 3) & s1_bmask
             s1_bmask = (((cmask >> J->stage1_shift) >> 3) & ~3u);
@@ -433,6 +434,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             s_fnl[tid] = LLONG_MAX;
             s_lnl[tid] = -1;
         } else {
+            // A stream past the job's end reads zero-filled rows (no '\n'): a last newline far ahead keeps all
+            // its windows invalid, so the byte loop needs no separate `active` test.
+            if (!active) lnp = 1 << 29;
             const int lnp_in = lnp;
             qn = 0;
             if (lane == 0)
@@ -466,9 +470,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                     if constexpr (MODE == 0) {
                         const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
                         const uint32_t w1 = lds32(s1 + ((hh >> 3) & s1_bmask));
-                        const bool b0 = (__funnelshift_r(w0, w0, hl) & 1u) != 0;
-                        const bool b1 = (__funnelshift_r(w1, w1, hh) & 1u) != 0;
-                        const bool pass = active && (j - lnp >= L) && b0 && (b1 || !two);
+                        // both table bits in one test (the second is forced on when S = 1)
+                        const uint32_t t = __funnelshift_r(w0, w0, hl) & (__funnelshift_r(w1, w1, hh) | one_probe);
+                        const bool pass = (j - lnp >= L) && (t & 1u) != 0;
                         enqueue(pass, (uint32_t)(kRowBytes + 32 * b + j), hl, hh, s1_first);
                     } else {
                         const int slot = j % kRing;
@@ -482,7 +486,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                         ring2_l[slot] = ring_l[slot];
                         ring2_h[slot] = ring_h[slot];
                         ring2_v[slot] = ldg_if(main_words + (((ring_h[slot] & p2_mask) + p2_add) >> 5), pass1);
-                        const bool valid = active && (j - lnp >= L);
+                        const bool valid = j - lnp >= L;
                         ring_l[slot] = hl;
                         ring_h[slot] = hh;
                         ring_v[slot] = ldg_if(main_words + ((hl & cmask) >> 5), valid);
