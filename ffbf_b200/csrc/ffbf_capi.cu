@@ -355,6 +355,14 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
         cudaGetLastError();
         return bail(FFBF_ECUDA);
     }
+    {
+        size_t fr = 0, tot = 0;
+        if (cudaMemGetInfo(&fr, &tot) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(FFBF_ECUDA);
+        }
+        c->device_mem = tot;
+    }
     if (dalloc_t(c, &c->d_main, c->filter_bytes / 4) || dalloc_t(c, &c->d_ff, c->filter_bytes / 4) ||
         dalloc_t(c, &c->d_counters, ffbf::CNT_WORDS))
         return bail(FFBF_ENOMEM_DEVICE);
@@ -826,6 +834,9 @@ ffbf_status segment_size(ffbf_ctx* c, uint64_t len, uint64_t* seg) {
     if (c->budget) {
         avail = c->budget > c->used ? c->budget - c->used : 0;
     } else {
+        // asking the driver for free memory costs about a millisecond: only texts of a quarter of the
+        // device or more can fail to fit, so smaller ones skip the query
+        if (scan_need(c, len) < c->device_mem / 4) return FFBF_OK;
         size_t fr = 0, tot = 0;
         CUDA_TRY(c, cudaMemGetInfo(&fr, &tot));
         avail = fr > (1ull << 30) ? fr - (1ull << 30) : 0;

@@ -28,6 +28,7 @@ struct ffbf_ctx {
     ffbf::Geom g{};
     int device = 0;
     int num_sms = 0;
+    uint64_t device_mem = 0;  // the device's total memory
     cudaStream_t st = nullptr;
     uint64_t budget = 0, used = 0;
     std::map<void*, size_t> allocs;

@@ -521,26 +521,70 @@ __global__ void __launch_bounds__(1024) k_tile_scan2(const long long* first, con
     }
 }
 
+// Byte masks of '\n' in a 32-bit word (0x80 in each byte that is '\n'; no false positives).
+__device__ __forceinline__ uint32_t nl_bytes(uint32_t w) {
+    const uint32_t t = w ^ 0x0A0A0A0Au;
+    return ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
+}
+
+// Last '\n' in [lo, p] (p >= lo), or -1: aligned 16-byte chunks from p down to lo.
+__device__ __forceinline__ long long last_nl_back(const uint8_t* text, long long lo, long long p) {
+    while (p >= lo) {
+        const long long c = p & ~15LL;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(text + c));
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        // bytes of the chunk at offsets max(lo - c, 0) .. p - c
+        const int hi = (int)(p - c), low = (int)max(lo - c, 0LL);
+        for (int q = hi >> 2; q >= (low >> 2); q--) {
+            uint32_t m = nl_bytes(w[q]);
+            // keep byte positions 4q + b with low <= 4q + b <= hi
+            const int b_hi = min(hi - 4 * q, 3), b_lo = max(low - 4 * q, 0);
+            m &= (0xFFFFFFFFu >> (8 * (3 - b_hi))) & (0xFFFFFFFFu << (8 * b_lo));
+            if (m) return c + 4 * q + (31 - __clz(m)) / 8;
+        }
+        p = c - 1;
+    }
+    return -1;
+}
+
+// First '\n' in [q, hi) (q < hi), or -1: aligned 16-byte chunks from q up to hi.
+__device__ __forceinline__ long long first_nl_fwd(const uint8_t* text, long long q, long long hi) {
+    while (q < hi) {
+        const long long c = q & ~15LL;
+        const uint4 v = __ldg(reinterpret_cast<const uint4*>(text + c));
+        const uint32_t w[4] = {v.x, v.y, v.z, v.w};
+        const int low = (int)(q - c), top = (int)min(hi - c, 16LL) - 1;  // offsets low .. top
+        for (int k = low >> 2; k <= (top >> 2); k++) {
+            uint32_t m = nl_bytes(w[k]);
+            const int b_lo = max(low - 4 * k, 0), b_hi = min(top - 4 * k, 3);
+            m &= (0xFFFFFFFFu << (8 * b_lo)) & (0xFFFFFFFFu >> (8 * (3 - b_hi)));
+            if (m) return c + 4 * k + (__ffs(m) - 1) / 8;
+        }
+        q = c + 16;
+    }
+    return -1;
+}
+
 __global__ void k_resolve(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
                           const long long* prev_nl, const long long* next_nl, HitLine* out) {
     uint32_t j = blockIdx.x * blockDim.x + threadIdx.x;
     if (j >= nhits) return;
     const uint64_t w = hits[j].off;
+    // line start: the last '\n' before the window in its tile, else the tile summaries' prefix
     uint64_t s = 0;
     if (w > 0) {
-        uint64_t tb = (w - 1) / kScanTile;
-        long long p = (long long)w - 1, lo = (long long)(tb * kScanTile);
-        while (p >= lo && text[p] != '\n') p--;
-        if (p >= lo) s = (uint64_t)p + 1;
-        else s = (uint64_t)(prev_nl[tb] + 1);
+        const uint64_t tb = (w - 1) / kScanTile;
+        const long long p = last_nl_back(text, (long long)(tb * kScanTile), (long long)w - 1);
+        s = p >= 0 ? (uint64_t)p + 1 : (uint64_t)(prev_nl[tb] + 1);
     }
+    // line end: the first '\n' after the window in its tile, else the suffix summary, else the text's end
     uint64_t e = n;
-    uint64_t q = w + len;
+    const uint64_t q = w + len;
     if (q < n) {
-        uint64_t te = q / kScanTile;
-        uint64_t hi = min(n, (te + 1) * (uint64_t)kScanTile);
-        while (q < hi && text[q] != '\n') q++;
-        if (q < hi) e = q;
+        const uint64_t te = q / kScanTile;
+        const uint64_t hi = min(n, (te + 1) * (uint64_t)kScanTile);
+        const long long f = first_nl_fwd(text, (long long)q, (long long)hi);
+        if (f >= 0) e = (uint64_t)f;
         else e = next_nl[te] == LLONG_MAX ? n : (uint64_t)next_nl[te];
     }
     out[j] = HitLine{s, e};
@@ -549,7 +593,7 @@ __global__ void k_resolve(const uint8_t* text, uint64_t n, uint32_t len, const H
 cudaError_t resolve_lines(const uint8_t* text, uint64_t n, uint32_t len, const HitRec* hits, uint32_t nhits,
                           const long long* tile_first, const long long* tile_last, long long* prev_nl,
                           long long* next_nl, uint64_t ntiles, HitLine* out, cudaStream_t st, long long* agg) {
-    if (ntiles && agg && ntiles > kTileAggBlock) {
+    if (ntiles && agg) {
         const uint32_t nb = (uint32_t)((ntiles + kTileAggBlock - 1) / kTileAggBlock);
         k_tile_agg<<<nb, 1024, 0, st>>>(tile_first, tile_last, ntiles, agg, agg + nb);
         k_tile_scan2<<<nb, 1024, 0, st>>>(tile_first, tile_last, ntiles, agg, agg + nb, nb, prev_nl, next_nl);
@@ -623,6 +667,32 @@ cudaError_t table_build(const uint64_t* d_ids, uint64_t nids, const uint64_t* d_
 }
 
 // One thread per hit window: look its hash up, byte-compare every candidate pattern at the window start.
+// The 16 bytes at p (any alignment), of which the first `need` (1..16) are used, read as aligned 16-byte
+// loads: the chunk holding p, and the next one only when the bytes reach into it. An aligned chunk that holds a
+// needed byte never crosses a page, so no load leaves the buffer's pages.
+__device__ __forceinline__ uint4 load16_unaligned(const uint8_t* p, uint32_t need) {
+    const uintptr_t a = (uintptr_t)p;
+    const uint4* base = reinterpret_cast<const uint4*>(a & ~(uintptr_t)15);
+    const uint32_t off = (uint32_t)(a & 15);
+    const uint4 x0 = __ldg(base);
+    const uint4 x1 = off + need > 16 ? __ldg(base + 1) : make_uint4(0, 0, 0, 0);
+    const uint32_t ws = off >> 2, bs = (off & 3) * 8;
+    // words ws .. ws + 4 of x0:x1, selected without a runtime-indexed array
+    uint32_t w0, w1, w2, w3, w4;
+    if (ws == 0) { w0 = x0.x; w1 = x0.y; w2 = x0.z; w3 = x0.w; w4 = x1.x; }
+    else if (ws == 1) { w0 = x0.y; w1 = x0.z; w2 = x0.w; w3 = x1.x; w4 = x1.y; }
+    else if (ws == 2) { w0 = x0.z; w1 = x0.w; w2 = x1.x; w3 = x1.y; w4 = x1.z; }
+    else { w0 = x0.w; w1 = x1.x; w2 = x1.y; w3 = x1.z; w4 = x1.w; }
+    return make_uint4(__funnelshift_r(w0, w1, bs), __funnelshift_r(w1, w2, bs), __funnelshift_r(w2, w3, bs),
+                      __funnelshift_r(w3, w4, bs));
+}
+
+// mask of the bytes of 32-bit word i that fall within the first `need` bytes of a 16-byte block
+__device__ __forceinline__ uint32_t word_mask(uint32_t need, uint32_t i) {
+    const uint32_t v = need > 4 * i ? min(need - 4 * i, 4u) : 0u;
+    return v >= 4 ? 0xffffffffu : (1u << (8 * v)) - 1u;
+}
+
 __global__ void k_verify(const HitRec* hits, uint32_t nhits, const uint8_t* text, uint64_t n, const uint64_t* keys,
                          const uint32_t* vals, uint64_t mask, const uint8_t* pat, const uint64_t* pstart,
                          const uint64_t* pend, uint64_t* m_off, uint32_t* m_pid, uint32_t cap, uint32_t* counters) {
@@ -638,20 +708,15 @@ __global__ void k_verify(const HitRec* hits, uint32_t nhits, const uint8_t* text
             if (w + pl <= n) {
                 const uint8_t* t = text + w;
                 const uint8_t* q = pat + ps;
-                uint64_t k = 0;
-                // 8-byte compares while both sides allow an aligned-free byte gather
-                while (k + 8 <= pl) {
-                    uint64_t x = 0, y = 0;
-#pragma unroll
-                    for (int b = 0; b < 8; b++) {
-                        x |= (uint64_t)t[k + b] << (8 * b);
-                        y |= (uint64_t)q[k + b] << (8 * b);
-                    }
-                    if (x != y) break;
-                    k += 8;
+                // byte compare, 16 bytes per step from aligned 16-byte loads of both sides
+                bool same = true;
+                for (uint64_t k = 0; k < pl && same; k += 16) {
+                    const uint32_t need = pl - k < 16 ? (uint32_t)(pl - k) : 16u;
+                    const uint4 x = load16_unaligned(t + k, need), y = load16_unaligned(q + k, need);
+                    same = (((x.x ^ y.x) & word_mask(need, 0)) | ((x.y ^ y.y) & word_mask(need, 1)) |
+                            ((x.z ^ y.z) & word_mask(need, 2)) | ((x.w ^ y.w) & word_mask(need, 3))) == 0;
                 }
-                while (k < pl && t[k] == q[k]) k++;
-                if (k == pl) {
+                if (same) {
                     uint32_t o = atomicAdd(counters + CNT_MATCHES, 1u);
                     if (o < cap) {
                         m_off[o] = w;

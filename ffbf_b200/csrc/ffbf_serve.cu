@@ -429,7 +429,9 @@ void worker_loop(ffbf_server* s) {
             collect_slow(s);
             progress = true;
         }
-        if (!progress) std::this_thread::sleep_for(std::chrono::microseconds(10));
+        // Requests on the device or in copies: poll again at once (a sleep rounds up to tens of microseconds
+        // on every stage of a request); with nothing in flight the loop waits on cv_work above.
+        if (!progress) std::this_thread::yield();
     }
     // stopping: let the device finish what was issued, then drop what is left
     cudaStreamSynchronize(s->st_copy);
