@@ -647,7 +647,7 @@ def main_ours(args):
 
     # end-to-end through the public API from pinned host memory: per-step host times, the median reported
     # (the host's PCIe and memory are shared with other jobs on this machine, so single steps vary)
-    e2e_steps = args.e2e_steps or min(args.steps, 5)
+    e2e_steps = args.e2e_steps or max(5, min(args.steps, 10))
     barrier()
     d2h = 0
     e2e_times = []
