@@ -34,10 +34,11 @@ struct ffbf_batch {
         uint64_t tiles_cap;
         int threads, mode;
         uint32_t rows;
+        int order;
         bool operator==(const Key& o) const {
             return main == o.main && ff == o.ff && hits == o.hits && counters == o.counters && tiles == o.tiles &&
                    stage1 == o.stage1 && hits_cap == o.hits_cap && tiles_cap == o.tiles_cap && threads == o.threads &&
-                   mode == o.mode && rows == o.rows;
+                   mode == o.mode && rows == o.rows && order == o.order;
         }
     };
     std::vector<Key> keys;
@@ -86,7 +87,9 @@ ffbf_status build_plan(const std::vector<PlanJob>& jobs, int num_sms, ScanPlan& 
             if (fj.n_supertiles) {
                 Group* gp = nullptr;
                 for (auto& g : groups)
-                    if (g.len == c->g.len && g.cfg.mode == cfg.mode && ffbf::config_threads(g.cfg) == threads) gp = &g;
+                    if (g.len == c->g.len && g.cfg.mode == cfg.mode && ffbf::config_threads(g.cfg) == threads &&
+                        (cfg.mode == 0 || g.cfg.order == cfg.order))
+                        gp = &g;
                 if (!gp) {
                     groups.push_back(Group{c->g.len, cfg, {}});
                     gp = &groups.back();
@@ -157,7 +160,7 @@ ffbf_status autotune_impl(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
 ffbf_batch::Key batch_key(const ffbf_ctx* c) {
     return ffbf_batch::Key{c->d_main, c->d_ff,          c->d_hits,      c->d_counters, c->d_tiles,
                            c->d_stage1, c->hits_cap,    c->tiles_cap,   c->cfg.threads, c->cfg.mode,
-                           c->cfg.rows};
+                           c->cfg.rows, c->cfg.order};
 }
 
 ffbf_status bfail(ffbf_batch* b, ffbf_status s, const std::string& msg) {
@@ -414,7 +417,9 @@ ffbf_status autotune_impl(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
     uint32_t* saved = nullptr;
     TRY(dalloc_t(c, &saved, c->filter_bytes / 4));
     CUDA_TRY(c, cudaMemcpyAsync(saved, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
-    const ffbf::FastConfig cands[] = {{512, 0, 0}, {384, 0, 0}, {256, 0, 0}, {384, 1, 0}, {256, 1, 0}};
+    // shared-memory mode at three CTA sizes, dense mode at two (its probe order follows the filter's fills)
+    const ffbf::FastConfig cands[] = {{512, 0, 0, 0}, {384, 0, 0, 0}, {256, 0, 0, 0}, {384, 1, 0, 0},
+                                      {256, 1, 0, 0}};
     ffbf::FastConfig best = c->cfg;
     double best_score = 1e300;
     cudaEvent_t e0, e1;

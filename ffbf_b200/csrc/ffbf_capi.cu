@@ -169,7 +169,7 @@ const uint64_t kInitialHitsCap = 1u << 16;
 ffbf_status prepare_fast(ffbf_ctx* c) {
     if (c->borrowed) {
         // the filter's owner built the stage-1 table and chose the configuration
-        if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 1));
+        if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 3));
         if (!c->h_job) {
             if (cudaMallocHost(&c->h_job, sizeof(ffbf::FastJob)) != cudaSuccess) {
                 cudaGetLastError();
@@ -187,7 +187,7 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         dfree(c, c->d_stage1);
         c->stage1_dirty = true;
     }
-    if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 1));
+    if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 3));
     if (!c->h_job) {
         if (cudaMallocHost(&c->h_job, sizeof(ffbf::FastJob)) != cudaSuccess) {
             cudaGetLastError();
@@ -205,10 +205,15 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         CUDA_TRY(c, ffbf::build_stage1(c->d_main, c->g, sparse_threads, c->d_stage1, c->st));
         const uint32_t nw = ffbf::stage1_words_for(c->g, sparse_threads);
         CUDA_TRY(c, ffbf::popcount_words(c->d_stage1, nw, c->d_popc, c->st));
-        unsigned long long ones = 0;
-        CUDA_TRY(c, cudaMemcpyAsync(&ones, c->d_popc, sizeof ones, cudaMemcpyDeviceToHost, c->st));
+        // fills of the cache and external regions pick the dense mode's probe order
+        const uint32_t cw = c->g.cache_bits / 32, ew = (uint32_t)(((uint64_t)c->g.ext_mask + 1) / 32);
+        CUDA_TRY(c, ffbf::popcount_words(c->d_main, cw, c->d_popc + 1, c->st));
+        CUDA_TRY(c, ffbf::popcount_words(c->d_main + cw, ew, c->d_popc + 2, c->st));
+        unsigned long long ones[3] = {0, 0, 0};
+        CUDA_TRY(c, cudaMemcpyAsync(ones, c->d_popc, sizeof ones, cudaMemcpyDeviceToHost, c->st));
         TRY(sync(c));
-        c->stage1_fill = (double)ones / (32.0 * nw);
+        c->stage1_fill = (double)ones[0] / (32.0 * nw);
+        c->probe_order = ffbf::dense_probe_order(c->g, (double)ones[1] / (32.0 * cw), (double)ones[2] / (32.0 * ew));
         if (!c->cfg_tuned) {
             c->cfg.mode = c->force_mode >= 0 ? c->force_mode : c->stage1_fill > 0.3 ? 1 : 0;
             // default CTA sizes (measured best on the 10k- and 1M-pattern workloads): 512 threads for the
@@ -218,6 +223,11 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         c->stage1_dirty = false;
     }
     if (c->force_mode >= 0) c->cfg.mode = c->force_mode;
+    // the dense mode pipelines two probes of distinct index functions: with K = 1 only the sparse mode applies
+    if (c->g.k < 2) c->cfg.mode = 0;
+    // the dense mode's probe order is the filter's (from the region fills), unless the environment fixes it
+    c->cfg.order = c->force_order >= 0 ? c->force_order : c->probe_order;
+    if (c->g.k < 4) c->cfg.order = 0;  // order 1 probes f2 and f3 first
     return FFBF_OK;
 }
 
@@ -381,6 +391,8 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
     if (th && (atoi(th) == 256 || atoi(th) == 384 || atoi(th) == 512)) c->cfg.threads = c->threads_env = atoi(th);
     const char* fm = getenv("FFBF_SCAN_MODE");
     if (fm && (fm[0] == '0' || fm[0] == '1')) c->force_mode = fm[0] - '0';
+    const char* fo = getenv("FFBF_SCAN_ORDER");
+    if (fo && (fo[0] == '0' || fo[0] == '1')) c->force_order = fo[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");
     c->force_generic = fg && fg[0] == '1';
     *out = c;

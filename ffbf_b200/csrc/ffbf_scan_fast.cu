@@ -30,6 +30,7 @@
 #include <cuda.h>
 #include <cudaTypedefs.h>
 
+#include <algorithm>
 #include <climits>
 #include <cstring>
 
@@ -116,6 +117,13 @@ __device__ __forceinline__ void rol_pair(uint32_t lo, uint32_t hi, uint32_t& rlo
     }
 }
 
+// rol32 by a compile-time amount (0: identity)
+template <int N>
+__device__ __forceinline__ uint32_t rot_const(uint32_t x) {
+    if constexpr (N == 0) return x;
+    else return __funnelshift_l(x, x, N);
+}
+
 // Full test from probe FROM on (reference order, early exit); probes before FROM are known to be set.
 __device__ __forceinline__ bool full_check_from(const Geom& g, const uint32_t* __restrict__ words, uint64_t h,
                                                 uint32_t from) {
@@ -191,6 +199,9 @@ __device__ __noinline__ void flush_queue(const FastJob* J, uint32_t qaddr, int q
 // first two index functions are global loads issued per valid window and consumed kRing bytes later from
 // register rings, so L2 latency overlaps the hashing of the next windows; only windows whose two probed bits
 // are set go to the queue.
+// MODE 2: MODE 1 with the pipelined probes on index functions f2 = rot16(h1) and f3 = rot16(h2) (the
+// external region for S <= 2, usually much sparser than the cache region, so fewer windows need a second
+// probe); queued windows then run the whole K-bit test.
 template <int L, int THREADS, int MODE>
 __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
                                                           uint32_t n_items, uint32_t max_s1_words,
@@ -298,7 +309,8 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
 
     // the current job's parameters (reloaded when the job changes)
     int cur_job = -1;
-    uint32_t R = 0, cmask = 0, s1_bmask = 0, p2_mask = 0, p2_add = 0, s1_first = 0, spt_log2 = 0, one_probe = 0;
+    uint32_t R = 0, s1_bmask = 0, s1_first = 0, spt_log2 = 0, one_probe = 0;
+    uint32_t a_mask = 0, a_add = 0, b_mask = 0, b_add = 0;  // dense mode: regions of the two pipelined probes
     bool two = false;
     auto job_desc = [&]() { return jobs + cur_job; };
     // The filter pointer is held in a register: the loop's global stores would otherwise make the compiler
@@ -327,9 +339,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             }
         }
     };
-    // dense-mode rings. Stage A: the h1-probe word (0 when the window was not valid, so its test fails),
+    // dense-mode rings. Stage A: the first probe's word (0 when the window was not valid, so its test fails),
     // h1, h2. Stage B: the second probe's word (0 when stage A failed), h1, h2.
-    constexpr int kR = MODE == 1 ? kRing : 1;
+    constexpr int kR = MODE != 0 ? kRing : 1;
+    // dense mode: rotation of h1/h2 giving the pipelined probes' index functions, and the first probe a
+    // queued window still needs in the reference order (MODE 1 knows f0 and f1; MODE 2 retests all)
+    constexpr int kRot = MODE == 2 ? 16 : 0;
+    constexpr uint32_t kFirstB = MODE == 2 ? 0u : 2u, kFirstA = MODE == 2 ? 0u : 1u;
     uint32_t ring_v[kR], ring_l[kR], ring_h[kR], ring2_v[kR], ring2_l[kR], ring2_h[kR];
 #pragma unroll
     for (int q = 0; q < kR; q++) ring_v[q] = ring_l[q] = ring_h[q] = ring2_v[q] = ring2_l[q] = ring2_h[q] = 0;
@@ -372,15 +388,16 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             spt_log2 = J->streams_per_tile_log2;
             main_words = J->main_words;
             s1_fits = MODE != 0 || J->stage1_nwords <= max_s1_words;
-            cmask = g.cache_mask;
+            const uint32_t cmask = g.cache_mask;
             two = g.s > 1;
             one_probe = two ? 0u : 1u;
             // stage-1 table of T = C >> shift bits, folded modulo T: the byte offset of bit (h & (T-1))'s
             // word is (h >> 3) & s1_bmask
             s1_bmask = (((cmask >> J->stage1_shift) >> 3) & ~3u);
-            // second probe's index function (getHashValue case 1): cache region when S > 1, else external
-            p2_mask = two ? cmask : g.ext_mask;
-            p2_add = two ? 0u : g.cache_bits;
+            a_mask = J->a_mask;
+            a_add = J->a_add;
+            b_mask = J->b_mask;
+            b_add = J->b_add;
             // sparse mode: the stage-1 probes are exact when the table is the cache region itself
             s1_first = J->stage1_shift == 0 ? (two ? 2u : 1u) : 0u;
             if constexpr (MODE == 0) {
@@ -476,20 +493,27 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                         enqueue(pass, (uint32_t)(kRowBytes + 32 * b + j), hl, hh, s1_first);
                     } else {
                         const int slot = j % kRing;
-                        // stage B: the window that entered stage A 2*kRing bytes ago
-                        // (the second probe's bit sits at h2 & 31 in its word for both index functions)
-                        const bool pass2 = (__funnelshift_r(ring2_v[slot], ring2_v[slot], ring2_h[slot]) & 1u) != 0;
+                        // stage B: the window that entered stage A 2*kRing bytes ago (a probe's bit sits at
+                        // f & 31 in its word: region offsets are multiples of 32)
+                        const uint32_t fb_old = rot_const<kRot>(ring2_h[slot]);
+                        const bool pass2 = (__funnelshift_r(ring2_v[slot], ring2_v[slot], fb_old) & 1u) != 0;
                         enqueue(pass2, (uint32_t)(kRowBytes + 32 * b + j - 2 * kRing), ring2_l[slot], ring2_h[slot],
-                                2u);
-                        // stage A: the window issued kRing bytes ago; its h1 word has arrived by now
-                        const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], ring_l[slot]) & 1u) != 0;
+                                kFirstB);
+                        // stage A: the window issued kRing bytes ago; its word has arrived by now
+                        const uint32_t fa_old = rot_const<kRot>(ring_l[slot]);
+                        const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], fa_old) & 1u) != 0;
                         ring2_l[slot] = ring_l[slot];
                         ring2_h[slot] = ring_h[slot];
-                        ring2_v[slot] = ldg_if(main_words + (((ring_h[slot] & p2_mask) + p2_add) >> 5), pass1);
+                        const uint32_t fb = rot_const<kRot>(ring_h[slot]);
+                        ring2_v[slot] = ldg_if(main_words + (((fb & b_mask) + b_add) >> 5), pass1);
                         const bool valid = j - lnp >= L;
                         ring_l[slot] = hl;
                         ring_h[slot] = hh;
-                        ring_v[slot] = ldg_if(main_words + ((hl & cmask) >> 5), valid);
+                        const uint32_t fa = rot_const<kRot>(hl);
+                        if constexpr (MODE == 1)  // f0 is in the cache region (S >= 1): no offset
+                            ring_v[slot] = ldg_if(main_words + ((fa & a_mask) >> 5), valid);
+                        else
+                            ring_v[slot] = ldg_if(main_words + (((fa & a_mask) + a_add) >> 5), valid);
                     }
                 }
                 if (lnp != lnp_blk && row_first < 0 && need_first) {
@@ -503,7 +527,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
 #pragma unroll
                 for (int q = 0; q < 8; q++) prev[q] = cur[q];
             }
-            if constexpr (MODE == 1) {
+            if constexpr (MODE != 0) {
                 // The rings carry over into the stream's next row (whose bytes follow this row's); at the
                 // stream's end they drain: stage-B slot q holds the window ending at 128 - 2*kRing + q,
                 // stage-A slot q the one at 128 - kRing + q; stage-A survivors go to the queue with only
@@ -511,10 +535,12 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                 if ((uint32_t)r == R - 1) {
 #pragma unroll
                     for (int q = 0; q < kRing; q++) {
-                        const bool pass2 = (__funnelshift_r(ring2_v[q], ring2_v[q], ring2_h[q]) & 1u) != 0;
-                        enqueue(pass2, (uint32_t)(2 * kRowBytes - 2 * kRing + q), ring2_l[q], ring2_h[q], 2u);
-                        const bool pass1 = (__funnelshift_r(ring_v[q], ring_v[q], ring_l[q]) & 1u) != 0;
-                        enqueue(pass1, (uint32_t)(2 * kRowBytes - kRing + q), ring_l[q], ring_h[q], 1u);
+                        const uint32_t fb = rot_const<kRot>(ring2_h[q]);
+                        const bool pass2 = (__funnelshift_r(ring2_v[q], ring2_v[q], fb) & 1u) != 0;
+                        enqueue(pass2, (uint32_t)(2 * kRowBytes - 2 * kRing + q), ring2_l[q], ring2_h[q], kFirstB);
+                        const uint32_t fa = rot_const<kRot>(ring_l[q]);
+                        const bool pass1 = (__funnelshift_r(ring_v[q], ring_v[q], fa) & 1u) != 0;
+                        enqueue(pass1, (uint32_t)(2 * kRowBytes - kRing + q), ring_l[q], ring_h[q], kFirstA);
                         ring_v[q] = 0;
                         ring2_v[q] = 0;
                     }
@@ -593,9 +619,13 @@ cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
 template <int L>
 cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
                        uint32_t max_s1_words, uint32_t* d_ctl, int num_sms, cudaStream_t st) {
-    if (cfg.mode == 1)  // dense: 384 threads (ring depth 4) or 256 (depth 8); 512 would spill
+    if (cfg.mode == 1) {  // dense: 384 threads (ring depth 4) or 256 (depth 8); 512 would spill
+        if (cfg.order == 1)
+            return cfg.threads == 256 ? launch_cfg<L, 256, 2>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
+                                      : launch_cfg<L, 384, 2>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
         return cfg.threads == 256 ? launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
                                   : launch_cfg<L, 384, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
+    }
     switch (cfg.threads) {
         case 256: return launch_cfg<L, 256, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
         case 384: return launch_cfg<L, 384, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
@@ -633,6 +663,20 @@ uint32_t stage1_shift_for(const Geom& g, int threads) {
 
 uint32_t stage1_words_for(const Geom& g, int threads) {
     return (uint32_t)(((uint64_t)g.cache_bits >> stage1_shift_for(g, threads)) / 32);
+}
+
+int dense_probe_order(const Geom& g, double cache_fill, double ext_fill) {
+    if (g.k < 4) return 0;
+    // Cost of a pair (A, B) per valid window, in L2 probes: A always, B when A passes, and a queued
+    // window's full test (about three probes' worth of issue and flush work) when both pass. A probe of a
+    // region that the L1 left beside the shared memory can largely hold (about 64 KiB) mostly hits there.
+    const double c_bytes = g.cache_bits / 8.0, e_bytes = (g.ext_mask + 1.0) / 8.0;
+    auto fill = [&](uint32_t i) { return i < g.s ? cache_fill : ext_fill; };
+    auto miss = [&](uint32_t i) { return 1.0 - std::min(1.0, 65536.0 / (i < g.s ? c_bytes : e_bytes)); };
+    auto cost = [&](uint32_t a, uint32_t b) {
+        return miss(a) + fill(a) * miss(b) + 3.0 * fill(a) * fill(b);
+    };
+    return cost(2, 3) < cost(0, 1) ? 1 : 0;
 }
 
 int config_threads(const FastConfig& cfg) {
@@ -673,6 +717,16 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
     job->stage1_words = stage1_words;
     job->stage1_shift = cfg.mode != 0 ? 0 : stage1_shift_for(a.g, threads);
     job->stage1_nwords = cfg.mode != 0 ? 0 : (uint32_t)(((uint64_t)a.g.cache_bits >> job->stage1_shift) / 32);
+    {
+        // dense mode: regions of the pipelined probes, index functions f0/f1 (order 0) or f2/f3 (order 1,
+        // which only K >= 4 filters set)
+        if (cfg.mode != 0 && (a.g.k < 2 || (cfg.order == 1 && a.g.k < 4))) *err = cudaErrorInvalidValue;
+        const uint32_t fa = cfg.order == 1 ? 2u : 0u, fb = fa + 1;
+        job->a_mask = fa < a.g.s ? a.g.cache_mask : a.g.ext_mask;
+        job->a_add = fa < a.g.s ? 0u : a.g.cache_bits;
+        job->b_mask = fb < a.g.s ? a.g.cache_mask : a.g.ext_mask;
+        job->b_add = fb < a.g.s ? 0u : a.g.cache_bits;
+    }
     job->hits = a.hits;
     job->hits_cap = a.hits_cap;
     job->counters = a.counters;

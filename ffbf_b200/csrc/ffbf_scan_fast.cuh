@@ -21,6 +21,9 @@ struct alignas(64) FastJob {
     const uint32_t* stage1_words;  // sparse mode: cache region copy or its fold (global), copied into smem
     uint32_t stage1_nwords;
     uint32_t stage1_shift;         // the table holds C >> shift bits (0: exact copy of the cache region)
+    // dense mode: the regions of its two pipelined probes (bit = (f & mask) + add for index functions f0/f1,
+    // or f2/f3 when the configuration's probe order is 1)
+    uint32_t a_mask, a_add, b_mask, b_add;
     HitRec* hits;
     uint32_t hits_cap;
     uint32_t ready_spins;  // polls of *ready before the launch gives up (about 1 us each)
@@ -34,12 +37,21 @@ struct alignas(64) FastJob {
 };
 
 // How a job is scanned: CTA size (256/384/512), probe mode (0: sparse, shared-memory stage 1; 1: dense,
-// pipelined L2 probes), rows per stream (0: chosen from the text size).
+// pipelined L2 probes), rows per stream (0: chosen from the text size), and in the dense mode the probe order
+// (0: the pipelined probes are index functions f0 = h1 and f1 = h2; 1: f2 = rot16(h1) and f3 = rot16(h2),
+// the better pair when their region is sparser). The order only changes which bits are tested first: a
+// window hits iff all K bits are set, in any order.
 struct FastConfig {
     int threads;
     int mode;
     uint32_t rows;
+    int order;
 };
+
+// Probe order for the dense mode from the fills (fraction of set bits) of the cache and external regions:
+// the pair whose first probe passes least often, counting the second probe's pass rate too. Order 1 needs
+// f2 and f3 among the K index functions (K >= 4).
+int dense_probe_order(const Geom& g, double cache_fill, double ext_fill);
 
 // True when the tuned kernel handles this geometry and text size; otherwise the generic scan runs.
 bool fast_scan_supported(const Geom& g, uint64_t n);

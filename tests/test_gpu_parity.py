@@ -179,19 +179,23 @@ SCAN_VARIANTS = [
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "256"},
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "384"},
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "512"},
-    {"FFBF_SCAN_MODE": "1"},
-    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_THREADS": "256"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0", "FFBF_SCAN_THREADS": "256"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"},
 ]
+SCAN_ENV = ("FFBF_FORCE_GENERIC_SCAN", "FFBF_SCAN_MODE", "FFBF_SCAN_THREADS", "FFBF_SCAN_ORDER")
 
 
 @pytest.mark.parametrize("name", ["plain_small", "scale_small", "smem_cache", "edge_chunks", "binary_small",
                                   "dense_fp", "len19_default"])
 def test_scan_variants_agree_with_oracle(name, monkeypatch):
-    """Every scan kernel variant (generic; tuned sparse at each CTA size; tuned dense) is bit-exact."""
+    """Every scan kernel variant (generic; tuned sparse at each CTA size; tuned dense in both probe orders)
+    is bit-exact."""
     prm, pats, text = build_inputs(name)
     o, s, _, _, _ = run_oracle(prm, pats, text)
     for env in SCAN_VARIANTS:
-        for k in ("FFBF_FORCE_GENERIC_SCAN", "FFBF_SCAN_MODE", "FFBF_SCAN_THREADS"):
+        for k in SCAN_ENV:
             monkeypatch.delenv(k, raising=False)
         for k, v in env.items():
             monkeypatch.setenv(k, v)
@@ -202,6 +206,40 @@ def test_scan_variants_agree_with_oracle(name, monkeypatch):
             np.testing.assert_array_equal(r.line_start, s["line_start"], err_msg=str(env))
             np.testing.assert_array_equal(r.line_end, s["line_end"], err_msg=str(env))
             np.testing.assert_array_equal(f.get_filters()[1], o.ff, err_msg=str(env))
+    monkeypatch.setenv("FFBF_SCAN_THREADS", "0")
+    with Filter(prm):
+        pass  # restores the default CTA size for later tests
+
+
+@pytest.mark.parametrize("L,k,s", [(20, 1, 1), (20, 2, 1), (20, 2, 2), (24, 3, 1), (24, 4, 3), (24, 4, 4),
+                                   (32, 5, 1), (16, 6, 2), (19, 11, 0)])
+def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
+    """The dense mode pipelines two probes: f0/f1 (order 0) or f2/f3 (order 1, K >= 4). Each geometry's
+    regions decide where those probes land (cache or external) and which queued windows still need which
+    probes; K = 1 has no second index function and falls back to the shared-memory mode."""
+    from cases import _gen
+    from ffbf_b200 import datagen as dg
+    prm = Params(L, k, s, 1 << 14, 1 << 16)  # small regions: dense fills, many false positives
+    pats, text = _gen(40 + k * 3 + s, dg.PRINTABLE, 3000, L, L + 16, 2_000_000, 80, 300)
+    o, so, _, _, _ = run_oracle(prm, pats, text)
+    variants = [{}, {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
+                {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
+                {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"}]
+    for env in variants:
+        for key in SCAN_ENV:
+            monkeypatch.delenv(key, raising=False)
+        for key, v in env.items():
+            monkeypatch.setenv(key, v)
+        with Filter(prm) as f:
+            f.add_patterns(pats)
+            r = f.process(text)
+            np.testing.assert_array_equal(r.hit_offsets, so["hits"], err_msg=str(env))
+            np.testing.assert_array_equal(r.line_start, so["line_start"], err_msg=str(env))
+            np.testing.assert_array_equal(f.get_filters()[1], o.ff, err_msg=str(env))
+            if k < 2:
+                assert f.config()[1] == 0, "K = 1 must not run the dense mode"
+    for key in SCAN_ENV:
+        monkeypatch.delenv(key, raising=False)
     monkeypatch.setenv("FFBF_SCAN_THREADS", "0")
     with Filter(prm):
         pass  # restores the default CTA size for later tests
