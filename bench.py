@@ -133,16 +133,35 @@ def gpu_id_for(dev):
         return vis.split(",")[dev] if vis else dev
 
 
-def profiled_traffic_ratio(workload_name):
-    """DRAM bytes per text byte of the scan kernel, from the committed ncu summary for this workload."""
+def profiled_value(workload_name, row):
+    """A per-text-byte figure of the scan kernel (table row `row`) from the committed ncu summary for this
+    workload: traffic_bytes_per_text_byte (DRAM bytes) or l2_probes_per_text_byte (L2 requests)."""
     paths = [os.path.join(ROOT, "profiles", f"k_scan_fast_{m}_{workload_name}_256MiB.md") for m in ("dense", "sparse")]
     path = next((q for q in paths if os.path.exists(q)), None)
     if path is None:
         return None
     for line in open(path):
-        if line.startswith("| traffic_bytes_per_text_byte |"):
+        if line.startswith(f"| {row} |"):
             return float(line.split("|")[2])
     return None
+
+
+def profiled_traffic_ratio(workload_name):
+    return profiled_value(workload_name, "traffic_bytes_per_text_byte")
+
+
+PROBE_CEILING = 1.0  # random 4-byte L2 probes per clock per SM, measured on this pool's B200s
+
+
+def probe_bound(workload_name, gbs, sm_mhz, n_sms):
+    """The dense scan's real limit: random L2 probes of the filter, issued through the L1TEX unit."""
+    per_byte = profiled_value(workload_name, "l2_probes_per_text_byte")
+    if per_byte is None or not sm_mhz:
+        return None
+    achieved = per_byte * gbs * 1e9 / (n_sms * sm_mhz * 1e6)
+    return {"unit": "L2 probes/clk/SM", "achieved": achieved, "ceiling": PROBE_CEILING, "frac": achieved / PROBE_CEILING,
+            "probes_per_text_byte": per_byte, "sms": n_sms, "sm_mhz": sm_mhz,
+            "source": "probes per byte from the ncu summary in profiles/; ceiling from a random-probe microbenchmark"}
 
 
 L2_FLUSH_BYTES = 256 << 20  # about twice the 126 MB L2
@@ -706,7 +725,9 @@ def main_ours(args):
                      "peak_source": f"{peak_kind} hbm_gbs",
                      "traffic": (lambda r: None if r is None else r * n)(profiled_traffic_ratio(wl.name)),
                      "traffic_source": "ncu dram bytes of a 256 MiB capture scaled to this text (profiles/)",
-                     "algorithmic_bytes_per_launch": n},
+                     "algorithmic_bytes_per_launch": n,
+                     "probe_bound": probe_bound(wl.name, achieved, clocks.get("sm_mhz"),
+                                                torch.cuda.get_device_properties(dev).multi_processor_count)},
         "e2e": {"value": world * n / e2e_s / 1e9, "unit": UNIT, "h2d_bytes_per_step": n,
                 "d2h_bytes_per_step": d2h // max(e2e_steps, 1),
                 "api": "ffbf_scan + ffbf_prune + ffbf_verify from pinned host memory",
