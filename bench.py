@@ -436,8 +436,9 @@ def run_batched(args, local):
         "bit_exact": {"plain_streams_vs_plain": same(got_streams, ref), "batched_vs_plain": same(got_batch, ref)},
         "setup_s": {"generate_and_build": gen_s, "autotune": tune_s, "batch_prepare": prepare_s},
         "autotune_classes": n_classes,
-        "configs": dict(collections.Counter(f"{'dense' if f.config()[1] else 'sparse'}-{f.config()[0]}"
-                                            for f in filters)),
+        "configs": dict(collections.Counter(
+            (f"dense-{f.config()[0]}-order{f.probe_order()}" if f.config()[1] else f"sparse-{f.config()[0]}")
+            for f in filters)),
         "timing": "host clock between device-idle points, median of steps; batched_device = CUDA events",
     }
     b.close()

@@ -163,30 +163,25 @@ void reset_scan(ffbf_ctx* c) {
 
 const uint64_t kInitialHitsCap = 1u << 16;
 
-// Makes the tuned scan ready for this context's filter: the stage-1 table for the configured CTA size and,
-// unless the autotuner or the environment fixed it, the probe mode from the table's fill (the shared-memory
-// stage only pays while it rejects most windows).
+// Builds the stage-1 table for a CTA size and layout (the sparse mode's, or the dense mode's prefilter, which
+// has the room the dense kernel leaves) unless the table on the device already is that one.
+ffbf_status ensure_stage1(ffbf_ctx* c, int threads, bool dense, bool force) {
+    if (!force && c->d_stage1 && c->stage1_threads == threads && c->stage1_dense == dense) return FFBF_OK;
+    const uint32_t nw = ffbf::stage1_words_for(c->g, threads, dense);
+    if (c->d_stage1 && c->stage1_words != nw) dfree(c, c->d_stage1);
+    if (!c->d_stage1) TRY(dalloc_t(c, &c->d_stage1, nw));
+    c->stage1_words = nw;
+    c->stage1_threads = threads;
+    c->stage1_dense = dense;
+    CUDA_TRY(c, ffbf::build_stage1(c->d_main, c->g, threads, dense, c->d_stage1, c->st));
+    return FFBF_OK;
+}
+
+// Makes the tuned scan ready for this context's filter: the stage-1 table the configured kernel reads and,
+// unless the autotuner or the environment fixed them, the probe mode (from the sparse table's fill: the
+// shared-memory stage only pays while it rejects most windows) and the dense mode's probe order (from the
+// fills of the filter's regions).
 ffbf_status prepare_fast(ffbf_ctx* c) {
-    if (c->borrowed) {
-        // the filter's owner built the stage-1 table and chose the configuration
-        if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 3));
-        if (!c->h_job) {
-            if (cudaMallocHost(&c->h_job, sizeof(ffbf::FastJob)) != cudaSuccess) {
-                cudaGetLastError();
-                c->h_job = nullptr;
-                return fail(c, FFBF_ENOMEM_HOST, "pinned job descriptor");
-            }
-        }
-        if (!c->d_job) TRY(dalloc_t(c, &c->d_job, 1));
-        return FFBF_OK;
-    }
-    // the table is sized for the configured CTA; in the dense mode it only measures the filter's fill, so
-    // the table already built is kept
-    const int sparse_threads = c->cfg.mode != 0 && c->d_stage1 ? c->stage1_threads : c->cfg.threads;
-    if (c->d_stage1 && c->stage1_threads != sparse_threads) {
-        dfree(c, c->d_stage1);
-        c->stage1_dirty = true;
-    }
     if (!c->d_popc) TRY(dalloc_t(c, &c->d_popc, 3));
     if (!c->h_job) {
         if (cudaMallocHost(&c->h_job, sizeof(ffbf::FastJob)) != cudaSuccess) {
@@ -196,23 +191,19 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         }
     }
     if (!c->d_job) TRY(dalloc_t(c, &c->d_job, 1));
-    if (!c->d_stage1) {
-        TRY(dalloc_t(c, &c->d_stage1, ffbf::stage1_words_for(c->g, sparse_threads)));
-        c->stage1_threads = sparse_threads;
-        c->stage1_dirty = true;
-    }
-    if (c->stage1_dirty) {
-        CUDA_TRY(c, ffbf::build_stage1(c->d_main, c->g, sparse_threads, c->d_stage1, c->st));
-        const uint32_t nw = ffbf::stage1_words_for(c->g, sparse_threads);
-        CUDA_TRY(c, ffbf::popcount_words(c->d_stage1, nw, c->d_popc, c->st));
-        // fills of the cache and external regions pick the dense mode's probe order
+    if (c->borrowed) return FFBF_OK;  // the filter's owner built the table and chose the configuration
+    if (c->stage1_dirty || !c->d_stage1) {
+        // measured on the sparse table of the configured CTA size (512 while the mode is open)
+        const int tm = c->cfg.mode == 0 ? ffbf::config_threads(c->cfg) : 512;
+        TRY(ensure_stage1(c, tm, false, true));
+        CUDA_TRY(c, ffbf::popcount_words(c->d_stage1, c->stage1_words, c->d_popc, c->st));
         const uint32_t cw = c->g.cache_bits / 32, ew = (uint32_t)(((uint64_t)c->g.ext_mask + 1) / 32);
         CUDA_TRY(c, ffbf::popcount_words(c->d_main, cw, c->d_popc + 1, c->st));
         CUDA_TRY(c, ffbf::popcount_words(c->d_main + cw, ew, c->d_popc + 2, c->st));
         unsigned long long ones[3] = {0, 0, 0};
         CUDA_TRY(c, cudaMemcpyAsync(ones, c->d_popc, sizeof ones, cudaMemcpyDeviceToHost, c->st));
         TRY(sync(c));
-        c->stage1_fill = (double)ones[0] / (32.0 * nw);
+        c->stage1_fill = (double)ones[0] / (32.0 * c->stage1_words);
         c->probe_order = ffbf::dense_probe_order(c->g, (double)ones[1] / (32.0 * cw), (double)ones[2] / (32.0 * ew));
         if (!c->cfg_tuned) {
             c->cfg.mode = c->force_mode >= 0 ? c->force_mode : c->stage1_fill > 0.3 ? 1 : 0;
@@ -225,9 +216,12 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
     if (c->force_mode >= 0) c->cfg.mode = c->force_mode;
     // the dense mode pipelines two probes of distinct index functions: with K = 1 only the sparse mode applies
     if (c->g.k < 2) c->cfg.mode = 0;
-    // the dense mode's probe order is the filter's (from the region fills), unless the environment fixes it
+    // the dense mode's probe order is the filter's, unless the environment fixes it
     c->cfg.order = c->force_order >= 0 ? c->force_order : c->probe_order;
-    if (c->g.k < 4) c->cfg.order = 0;  // order 1 probes f2 and f3 first
+    if (c->g.k < 4 && c->cfg.order == 1) c->cfg.order = 0;  // order 1 probes f2 and f3 first
+    // the table the configured kernel reads (a dense kernel without prefilter reads none)
+    if (c->cfg.mode == 0) TRY(ensure_stage1(c, ffbf::config_threads(c->cfg), false, false));
+    else if (c->cfg.order == 2) TRY(ensure_stage1(c, ffbf::config_threads(c->cfg), true, false));
     return FFBF_OK;
 }
 
@@ -392,7 +386,7 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
     const char* fm = getenv("FFBF_SCAN_MODE");
     if (fm && (fm[0] == '0' || fm[0] == '1')) c->force_mode = fm[0] - '0';
     const char* fo = getenv("FFBF_SCAN_ORDER");
-    if (fo && (fo[0] == '0' || fo[0] == '1')) c->force_order = fo[0] - '0';
+    if (fo && fo[0] >= '0' && fo[0] <= '2') c->force_order = fo[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");
     c->force_generic = fg && fg[0] == '1';
     *out = c;
@@ -437,6 +431,8 @@ void attach_filters(ffbf_ctx* slot, const ffbf_ctx* owner) {
     slot->d_ff = owner->d_ff;
     slot->d_stage1 = owner->d_stage1;
     slot->stage1_threads = owner->stage1_threads;
+    slot->stage1_dense = owner->stage1_dense;
+    slot->stage1_words = owner->stage1_words;
     slot->stage1_fill = owner->stage1_fill;
     slot->stage1_dirty = false;
     slot->cfg = owner->cfg;
@@ -1202,6 +1198,12 @@ ffbf_status ffbf_get_scan_config(const ffbf_ctx* c, int* threads, int* mode) {
     if (!c) return FFBF_EINVAL;
     if (threads) *threads = ffbf::config_threads(c->cfg);
     if (mode) *mode = c->cfg.mode;
+    return FFBF_OK;
+}
+
+ffbf_status ffbf_get_probe_order(const ffbf_ctx* c, int* order) {
+    if (!c || !order) return FFBF_EINVAL;
+    *order = c->cfg.order;
     return FFBF_OK;
 }
 

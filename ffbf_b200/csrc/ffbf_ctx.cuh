@@ -65,14 +65,16 @@ struct ffbf_ctx {
     uint32_t* d_stage1 = nullptr;  // stage-1 table of the tuned scan (cache copy or its fold)
     bool stage1_dirty = true;
     int stage1_threads = 0;        // CTA size the table was sized for
+    bool stage1_dense = false;     // sized for the dense kernel's room (its prefilter, probe order 2)
+    uint32_t stage1_words = 0;
     unsigned long long* d_popc = nullptr;
     double stage1_fill = 0;
     ffbf::FastConfig cfg{512, 0, 0, 0};  // tuned-scan configuration (mode from the stage-1 fill, or the autotuner)
     bool cfg_tuned = false;
     int threads_env = 0;           // FFBF_SCAN_THREADS=256|384|512 in the environment
     int force_mode = -1;           // FFBF_SCAN_MODE=0|1 in the environment
-    int force_order = -1;          // FFBF_SCAN_ORDER=0|1 in the environment (dense-mode probe order)
-    int probe_order = 0;           // dense-mode probe order chosen from the region fills
+    int force_order = -1;          // FFBF_SCAN_ORDER=0|1|2 in the environment (dense-mode probe order)
+    int probe_order = 0;           // dense-mode probe order chosen from the region fills (0, 1, 2)
     bool force_generic = false;    // FFBF_FORCE_GENERIC_SCAN=1 in the environment
     // A context whose filters (main, feed-forward, stage-1 table) belong to another context: a served
     // request's scan state attached to a resident pattern set. It never frees or rebuilds them.

@@ -32,6 +32,7 @@
 
 #include <algorithm>
 #include <climits>
+#include <cmath>
 #include <cstring>
 
 #include "ffbf_scan_fast.cuh"
@@ -202,6 +203,9 @@ __device__ __noinline__ void flush_queue(const FastJob* J, uint32_t qaddr, int q
 // MODE 2: MODE 1 with the pipelined probes on index functions f2 = rot16(h1) and f3 = rot16(h2) (the
 // external region for S <= 2, usually much sparser than the cache region, so fewer windows need a second
 // probe); queued windows then run the whole K-bit test.
+// MODE 3: MODE 1 with a shared-memory prefilter: the f0 load is issued only for windows whose bit in the
+// folded cache region (the stage-1 table, sized for the room this kernel leaves) is set, so filters whose
+// fold still rejects many windows issue that many fewer L2 probes.
 template <int L, int THREADS, int MODE>
 __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
                                                           uint32_t n_items, uint32_t max_s1_words,
@@ -387,7 +391,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             R = J->rows;
             spt_log2 = J->streams_per_tile_log2;
             main_words = J->main_words;
-            s1_fits = MODE != 0 || J->stage1_nwords <= max_s1_words;
+            s1_fits = (MODE != 0 && MODE != 3) || J->stage1_nwords <= max_s1_words;
             const uint32_t cmask = g.cache_mask;
             two = g.s > 1;
             one_probe = two ? 0u : 1u;
@@ -400,7 +404,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             b_add = J->b_add;
             // sparse mode: the stage-1 probes are exact when the table is the cache region itself
             s1_first = J->stage1_shift == 0 ? (two ? 2u : 1u) : 0u;
-            if constexpr (MODE == 0) {
+            if constexpr (MODE == 0 || MODE == 3) {
                 const uint32_t nw = s1_fits ? J->stage1_nwords : 0u;
                 const uint32_t* src = J->stage1_words;
                 for (uint32_t i = tid; i < nw; i += THREADS) s1p[i] = src[i];
@@ -506,14 +510,19 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                         ring2_h[slot] = ring_h[slot];
                         const uint32_t fb = rot_const<kRot>(ring_h[slot]);
                         ring2_v[slot] = ldg_if(main_words + (((fb & b_mask) + b_add) >> 5), pass1);
-                        const bool valid = j - lnp >= L;
+                        bool issue = j - lnp >= L;
+                        if constexpr (MODE == 3) {
+                            // the folded table's bit: clear means the cache bit of f0 is clear too
+                            const uint32_t w = lds32(s1 + ((hl >> 3) & s1_bmask));
+                            issue = issue && (__funnelshift_r(w, w, hl) & 1u) != 0;
+                        }
                         ring_l[slot] = hl;
                         ring_h[slot] = hh;
                         const uint32_t fa = rot_const<kRot>(hl);
-                        if constexpr (MODE == 1)  // f0 is in the cache region (S >= 1): no offset
-                            ring_v[slot] = ldg_if(main_words + ((fa & a_mask) >> 5), valid);
+                        if constexpr (MODE != 2)  // f0 is in the cache region (S >= 1): no offset
+                            ring_v[slot] = ldg_if(main_words + ((fa & a_mask) >> 5), issue);
                         else
-                            ring_v[slot] = ldg_if(main_words + (((fa & a_mask) + a_add) >> 5), valid);
+                            ring_v[slot] = ldg_if(main_words + (((fa & a_mask) + a_add) >> 5), issue);
                     }
                 }
                 if (lnp != lnp_blk && row_first < 0 && need_first) {
@@ -605,7 +614,7 @@ constexpr size_t fixed_smem() {
 template <int L, int THREADS, int MODE>
 cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items, uint32_t max_s1_words,
                        uint32_t* d_ctl, int num_sms, cudaStream_t st) {
-    const size_t smem = fixed_smem<THREADS, MODE>() + (MODE == 0 ? 4 * (size_t)max_s1_words : 0);
+    const size_t smem = fixed_smem<THREADS, MODE>() + (MODE == 0 || MODE == 3 ? 4 * (size_t)max_s1_words : 0);
     cudaError_t e =
         cudaFuncSetAttribute(k_scan_fast<L, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -623,6 +632,10 @@ cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_
         if (cfg.order == 1)
             return cfg.threads == 256 ? launch_cfg<L, 256, 2>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
                                       : launch_cfg<L, 384, 2>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
+        if (cfg.order == 2)
+            return cfg.threads == 256
+                       ? launch_cfg<L, 256, 3>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st)
+                       : launch_cfg<L, 384, 3>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
         return cfg.threads == 256 ? launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
                                   : launch_cfg<L, 384, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
     }
@@ -633,7 +646,8 @@ cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_
     }
 }
 
-size_t fixed_smem_for(int threads) {
+size_t fixed_smem_for(int threads, bool dense) {
+    if (dense) return threads == 256 ? fixed_smem<256, 1>() : fixed_smem<384, 1>();
     switch (threads) {
         case 256: return fixed_smem<256, 0>();
         case 384: return fixed_smem<384, 0>();
@@ -654,29 +668,42 @@ bool fast_scan_supported(const Geom& g, uint64_t n) {
 }
 
 // Largest power-of-two stage-1 table (in bits, <= C) that fits beside the fixed shared-memory layout.
-uint32_t stage1_shift_for(const Geom& g, int threads) {
-    const size_t room = kSmemLimit - fixed_smem_for(threads) - static_smem(threads) - 64;
+uint32_t stage1_shift_for(const Geom& g, int threads, bool dense) {
+    const size_t room = kSmemLimit - fixed_smem_for(threads, dense) - static_smem(threads) - 64;
     uint32_t sh = 0;
     while (((uint64_t)g.cache_bits >> sh) / 8 > room) sh++;
     return sh;
 }
 
-uint32_t stage1_words_for(const Geom& g, int threads) {
-    return (uint32_t)(((uint64_t)g.cache_bits >> stage1_shift_for(g, threads)) / 32);
+uint32_t stage1_words_for(const Geom& g, int threads, bool dense) {
+    return (uint32_t)(((uint64_t)g.cache_bits >> stage1_shift_for(g, threads, dense)) / 32);
 }
 
 int dense_probe_order(const Geom& g, double cache_fill, double ext_fill) {
-    if (g.k < 4) return 0;
-    // Cost of a pair (A, B) per valid window, in L2 probes: A always, B when A passes, and a queued
-    // window's full test (about three probes' worth of issue and flush work) when both pass. A probe of a
-    // region that the L1 left beside the shared memory can largely hold (about 64 KiB) mostly hits there.
+    // Cost of a plan per valid window, in L2 probes: the first probe always, the second when the first
+    // passes, and a queued window's full test (about three probes' worth of issue and flush work) when both
+    // pass. A probe of a region that the L1 left beside the shared memory can largely hold (about 64 KiB)
+    // mostly hits there.
     const double c_bytes = g.cache_bits / 8.0, e_bytes = (g.ext_mask + 1.0) / 8.0;
     auto fill = [&](uint32_t i) { return i < g.s ? cache_fill : ext_fill; };
     auto miss = [&](uint32_t i) { return 1.0 - std::min(1.0, 65536.0 / (i < g.s ? c_bytes : e_bytes)); };
     auto cost = [&](uint32_t a, uint32_t b) {
         return miss(a) + fill(a) * miss(b) + 3.0 * fill(a) * fill(b);
     };
-    return cost(2, 3) < cost(0, 1) ? 1 : 0;
+    int best = 0;
+    double best_cost = cost(0, 1);
+    if (g.k >= 4 && cost(2, 3) < best_cost) {
+        best = 1;
+        best_cost = cost(2, 3);
+    }
+    // Order 2: f0's load only where the folded cache region (the table the 384-thread dense kernel has room
+    // for) has its bit set, at about 0.15 probes' worth of shared-memory work per window. A table bit ORs
+    // C/T cache bits, so it is set with probability 1 - (1 - fill)^(C/T).
+    const double folds = (double)(1u << stage1_shift_for(g, 384, true));
+    const double fold_fill = 1.0 - std::pow(1.0 - cache_fill, folds);
+    const double c2 = 0.15 + fold_fill * miss(0) + fill(0) * miss(1) + 3.0 * fill(0) * fill(1);
+    if (c2 < best_cost) best = 2;
+    return best;
 }
 
 int config_threads(const FastConfig& cfg) {
@@ -715,12 +742,15 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
     job->main_words = a.main_words;
     job->ff_words = a.ff_words;
     job->stage1_words = stage1_words;
-    job->stage1_shift = cfg.mode != 0 ? 0 : stage1_shift_for(a.g, threads);
-    job->stage1_nwords = cfg.mode != 0 ? 0 : (uint32_t)(((uint64_t)a.g.cache_bits >> job->stage1_shift) / 32);
+    // the table the kernel reads: the sparse mode's, or the dense mode's prefilter (order 2)
+    const bool reads_table = cfg.mode == 0 || cfg.order == 2;
+    job->stage1_shift = reads_table ? stage1_shift_for(a.g, threads, cfg.mode != 0) : 0;
+    job->stage1_nwords = reads_table ? (uint32_t)(((uint64_t)a.g.cache_bits >> job->stage1_shift) / 32) : 0;
     {
         // dense mode: regions of the pipelined probes, index functions f0/f1 (order 0) or f2/f3 (order 1,
         // which only K >= 4 filters set)
-        if (cfg.mode != 0 && (a.g.k < 2 || (cfg.order == 1 && a.g.k < 4))) *err = cudaErrorInvalidValue;
+        if (cfg.mode != 0 && (a.g.k < 2 || (cfg.order == 1 && a.g.k < 4) || cfg.order < 0 || cfg.order > 2))
+            *err = cudaErrorInvalidValue;
         const uint32_t fa = cfg.order == 1 ? 2u : 0u, fb = fa + 1;
         job->a_mask = fa < a.g.s ? a.g.cache_mask : a.g.ext_mask;
         job->a_add = fa < a.g.s ? 0u : a.g.cache_bits;
@@ -801,8 +831,9 @@ __global__ void k_stage1_fold(const uint32_t* main_words, uint32_t sh, uint32_t*
     out[w] = v;
 }
 
-cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, int threads, uint32_t* out, cudaStream_t st) {
-    const uint32_t sh = stage1_shift_for(g, threads);
+cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, int threads, bool dense, uint32_t* out,
+                         cudaStream_t st) {
+    const uint32_t sh = stage1_shift_for(g, threads, dense);
     const uint32_t nwords = (uint32_t)(((uint64_t)g.cache_bits >> sh) / 32);
     if (sh == 0) return cudaMemcpyAsync(out, main_words, 4ull * nwords, cudaMemcpyDeviceToDevice, st);
     k_stage1_fold<<<(nwords + 255) / 256, 256, 0, st>>>(main_words, sh, out, nwords);

@@ -39,8 +39,9 @@ struct alignas(64) FastJob {
 // How a job is scanned: CTA size (256/384/512), probe mode (0: sparse, shared-memory stage 1; 1: dense,
 // pipelined L2 probes), rows per stream (0: chosen from the text size), and in the dense mode the probe order
 // (0: the pipelined probes are index functions f0 = h1 and f1 = h2; 1: f2 = rot16(h1) and f3 = rot16(h2),
-// the better pair when their region is sparser). The order only changes which bits are tested first: a
-// window hits iff all K bits are set, in any order.
+// the better pair when their region is sparser; 2: f0 and f1, with f0's load issued only when a folded copy
+// of the cache region in shared memory has its bit set). The order only changes which bits are tested
+// first: a window hits iff all K bits are set, in any order.
 struct FastConfig {
     int threads;
     int mode;
@@ -49,8 +50,8 @@ struct FastConfig {
 };
 
 // Probe order for the dense mode from the fills (fraction of set bits) of the cache and external regions:
-// the pair whose first probe passes least often, counting the second probe's pass rate too. Order 1 needs
-// f2 and f3 among the K index functions (K >= 4).
+// the plan with the fewest expected L2 probes per window. Order 1 needs f2 and f3 among the K index
+// functions (K >= 4).
 int dense_probe_order(const Geom& g, double cache_fill, double ext_fill);
 
 // True when the tuned kernel handles this geometry and text size; otherwise the generic scan runs.
@@ -58,11 +59,13 @@ bool fast_scan_supported(const Geom& g, uint64_t n);
 
 int config_threads(const FastConfig& cfg);
 
-// Stage-1 table of the sparse mode for a CTA size: a copy of the cache region when it fits in the shared
-// memory left over, otherwise its fold to C >> shift bits.
-uint32_t stage1_shift_for(const Geom& g, int threads);
-uint32_t stage1_words_for(const Geom& g, int threads);
-cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, int threads, uint32_t* out, cudaStream_t st);
+// Stage-1 table for a CTA size: a copy of the cache region when it fits in the shared memory the kernel
+// leaves over (the sparse kernel's, or with `dense` the dense kernel's, whose table prefilters f0 in probe
+// order 2), otherwise its fold to C >> shift bits.
+uint32_t stage1_shift_for(const Geom& g, int threads, bool dense = false);
+uint32_t stage1_words_for(const Geom& g, int threads, bool dense = false);
+cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, int threads, bool dense, uint32_t* out,
+                         cudaStream_t st);
 
 // Rows per stream for a text of n bytes, alone on the GPU or in a batch.
 uint32_t fast_rows(uint64_t n, int threads, int num_sms, bool batch);

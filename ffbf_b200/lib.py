@@ -37,7 +37,7 @@ EXPORTED = [
     "ffbf_test_line", "ffbf_clear_ff", "ffbf_get_filters", "ffbf_filter_bytes", "ffbf_free", "ffbf_format_spans",
     "ffbf_stream", "ffbf_kernel_launches", "ffbf_scan_static", "ffbf_batch_create", "ffbf_batch_add",
     "ffbf_batch_prepare", "ffbf_batch_launch", "ffbf_batch_wait", "ffbf_batch_stream", "ffbf_batch_last_error",
-    "ffbf_batch_destroy", "ffbf_batch_autotune", "ffbf_autotune", "ffbf_get_scan_config", "ffbf_debug_scan_unpublished", "ffbf_hashbench_lines", "ffbf_hashbench_file", "ffbf_host_alloc", "ffbf_host_free", "ffbf_server_create", "ffbf_server_add_set", "ffbf_server_submit",
+    "ffbf_batch_destroy", "ffbf_batch_autotune", "ffbf_autotune", "ffbf_get_scan_config", "ffbf_get_probe_order", "ffbf_debug_scan_unpublished", "ffbf_hashbench_lines", "ffbf_hashbench_file", "ffbf_host_alloc", "ffbf_host_free", "ffbf_server_create", "ffbf_server_add_set", "ffbf_server_submit",
     "ffbf_server_poll", "ffbf_server_release", "ffbf_server_get_stats", "ffbf_server_last_error",
     "ffbf_server_destroy",
 ]
@@ -152,6 +152,7 @@ def load_library(path=LIB_PATH):
         "ffbf_batch_destroy": (None, [vp]),
         "ffbf_batch_autotune": (ctypes.c_int, [vp, sz, P(ctypes.c_uint32)]),
         "ffbf_get_scan_config": (ctypes.c_int, [vp, P(ctypes.c_int), P(ctypes.c_int)]),
+        "ffbf_get_probe_order": (ctypes.c_int, [vp, P(ctypes.c_int)]),
         "ffbf_debug_scan_unpublished": (ctypes.c_int, [vp, vp, sz, ctypes.c_uint32]),
         "ffbf_hashbench_lines": (ctypes.c_int, [ctypes.c_int, vp, sz, P(u8p), P(sz)]),
         "ffbf_host_alloc": (vp, [sz]),
@@ -373,6 +374,12 @@ class Filter:
         t, m = ctypes.c_int(), ctypes.c_int()
         self._check(self._lib.ffbf_get_scan_config(self._h, ctypes.byref(t), ctypes.byref(m)))
         return t.value, m.value
+
+    def probe_order(self):
+        """The dense mode's probe plan (0: f0/f1; 1: f2/f3; 2: f0/f1 behind a shared-memory prefilter)."""
+        o = ctypes.c_int()
+        self._check(self._lib.ffbf_get_probe_order(self._h, ctypes.byref(o)))
+        return o.value
 
     def clear_ff(self):
         self._check(self._lib.ffbf_clear_ff(self._h))

@@ -264,6 +264,13 @@ ffbf_status ffbf_debug_scan_unpublished(ffbf_ctx* ctx, const uint8_t* d_text, si
  * it reports the defaults. */
 ffbf_status ffbf_get_scan_config(const ffbf_ctx* ctx, int* threads, int* mode);
 
+/* The dense mode's probe plan for this context's filter: 0 pipelines the loads of index functions f0 = h1
+ * and f1 = h2, 1 those of f2 = rot16(h1) and f3 = rot16(h2) (K >= 4), 2 those of f0 and f1 with f0's load
+ * skipped where a folded copy of the cache region in shared memory has its bit clear. Chosen from the
+ * fills of the filter's regions when the filter is prepared for a scan (FFBF_SCAN_ORDER=0|1|2 fixes it);
+ * a window hits iff all K bits are set, so the plan changes the work, never the result. */
+ffbf_status ffbf_get_probe_order(const ffbf_ctx* ctx, int* order);
+
 /* Zeroes the feed-forward filter (a fresh reverseBitvector, ffbf.cpp:107). Enqueued on the context's
  * stream; later calls on the context see it done. */
 ffbf_status ffbf_clear_ff(ffbf_ctx* ctx);

@@ -183,6 +183,8 @@ SCAN_VARIANTS = [
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0", "FFBF_SCAN_THREADS": "256"},
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "2"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "2", "FFBF_SCAN_THREADS": "256"},
 ]
 SCAN_ENV = ("FFBF_FORCE_GENERIC_SCAN", "FFBF_SCAN_MODE", "FFBF_SCAN_THREADS", "FFBF_SCAN_ORDER")
 
@@ -214,9 +216,10 @@ def test_scan_variants_agree_with_oracle(name, monkeypatch):
 @pytest.mark.parametrize("L,k,s", [(20, 1, 1), (20, 2, 1), (20, 2, 2), (24, 3, 1), (24, 4, 3), (24, 4, 4),
                                    (32, 5, 1), (16, 6, 2), (19, 11, 0)])
 def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
-    """The dense mode pipelines two probes: f0/f1 (order 0) or f2/f3 (order 1, K >= 4). Each geometry's
-    regions decide where those probes land (cache or external) and which queued windows still need which
-    probes; K = 1 has no second index function and falls back to the shared-memory mode."""
+    """The dense mode pipelines two probes: f0/f1 (order 0), f2/f3 (order 1, K >= 4), or f0/f1 behind a
+    shared-memory prefilter of f0 (order 2). Each geometry's regions decide where those probes land (cache or
+    external) and which queued windows still need which probes; K = 1 has no second index function and falls
+    back to the shared-memory mode."""
     from cases import _gen
     from ffbf_b200 import datagen as dg
     prm = Params(L, k, s, 1 << 14, 1 << 16)  # small regions: dense fills, many false positives
@@ -224,7 +227,8 @@ def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
     o, so, _, _, _ = run_oracle(prm, pats, text)
     variants = [{}, {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
-                {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"}]
+                {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"},
+                {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "2"}]
     for env in variants:
         for key in SCAN_ENV:
             monkeypatch.delenv(key, raising=False)
@@ -238,6 +242,12 @@ def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
             np.testing.assert_array_equal(f.get_filters()[1], o.ff, err_msg=str(env))
             if k < 2:
                 assert f.config()[1] == 0, "K = 1 must not run the dense mode"
+            if s < 1:
+                pass  # no cache-region probe: the generic scan runs and no probe plan is chosen
+            elif env.get("FFBF_SCAN_ORDER") == "1" and k < 4:
+                assert f.probe_order() == 0, "order 1 needs f2 and f3"
+            elif "FFBF_SCAN_ORDER" in env:
+                assert f.probe_order() == int(env["FFBF_SCAN_ORDER"])
     for key in SCAN_ENV:
         monkeypatch.delenv(key, raising=False)
     monkeypatch.setenv("FFBF_SCAN_THREADS", "0")
