@@ -53,6 +53,8 @@ def parse():
     ap.add_argument("--served-requests", type=int, default=4000, help="requests of the served workload")
     ap.add_argument("--served-rate", type=float, default=2000.0, help="Poisson arrival rate (requests/s)")
     ap.add_argument("--text-bytes", type=int, default=0, help="override the workload's text size")
+    ap.add_argument("--patterns", type=int, default=0,
+                    help="override the workload's pattern count (the line then names it, e.g. scale_200k)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (default: min(steps, 5))")
     ap.add_argument("--cpu-sample", type=int, default=1 << 30, help="bytes of text for the CPU baseline")
@@ -63,7 +65,16 @@ def parse():
 def workload(args):
     from ffbf_b200 import datagen as dg
     fn = {"scale": dg.scale, "plain": dg.plain, "binary": dg.binary}[args.workload]
-    return fn(args.text_bytes) if args.text_bytes else fn()
+    kw = {}
+    if args.text_bytes:
+        kw["text_bytes"] = args.text_bytes
+    if args.patterns:
+        kw["n_patterns"] = args.patterns
+    wl = fn(**kw)
+    if args.patterns:
+        # another pattern count is another workload: no committed profile describes it
+        wl.name = f"{wl.name}_{args.patterns // 1000}k"
+    return wl
 
 
 def describe(wl):
