@@ -144,6 +144,18 @@ public:
 
     ffbf_ctx* handle() { return ctx_; }
 
+    // The tuned scan's configuration as the filter's fills or ffbf_autotune chose it: CTA threads, mode (0
+    // shared-memory stage, 1 pipelined L2 probes) and the dense mode's probe order (0, 1 or 2).
+    struct ScanConfig {
+        int threads, mode, order;
+    };
+    ScanConfig scanConfig() {
+        ScanConfig c{0, 0, 0};
+        check(ffbf_get_scan_config(ctx_, &c.threads, &c.mode));
+        check(ffbf_get_probe_order(ctx_, &c.order));
+        return c;
+    }
+
     // The context with every queued pattern built into its filter, for the batch and server wrappers below.
     ffbf_ctx* built_handle() {
         flush();

@@ -61,6 +61,8 @@ int main(int argc, char** argv) {
         filter.processFile(0);
         ffbf_scan_result r = filter.collect();
         fprintf(stderr, "direct scan: %llu hits\n", (unsigned long long)r.n_hits);
+        const ffbf::Filter::ScanConfig sc = filter.scanConfig();
+        fprintf(stderr, "scan config: %d threads, mode %d, probe order %d\n", sc.threads, sc.mode, sc.order);
         std::ofstream out(argv[3]), idx(std::string("__index_") + argv[3]);
         int pfd = open(argv[2], O_RDONLY);
         filter.filterPhrases(pfd, out, idx);

@@ -355,6 +355,7 @@ def test_cpp_mirror_program_matches_reference_files(tmp_path):
         assert g.matches("pruned", (tmp_path / "out").read_bytes())
         assert g.matches("index", (tmp_path / "__index_out").read_bytes())
         direct = int(re.search(rb"direct scan: (\d+) hits", r.stderr).group(1))
+        assert re.search(rb"scan config: (256|384|512) threads, mode [01], probe order [012]", r.stderr), r.stderr
         if mode:
             served = int(re.search(rb"status 0, (\d+) hits", r.stderr).group(1))
             assert served == direct > 0
