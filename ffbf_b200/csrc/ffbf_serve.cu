@@ -52,6 +52,7 @@ struct Request {
 };
 
 constexpr uint64_t kArenaAlign = 256;
+constexpr uint64_t kSmallCopy = 4ull << 20;  // texts up to this size copy on the small-copy stream
 constexpr uint32_t kMaxCtl = 64;  // control-word groups per plan (one per tuned launch, plus one)
 constexpr uint64_t kPreallocText = 512ull << 20;  // request size the slots' scan buffers start out sized for
 constexpr uint32_t kPreallocHits = 16384;          // hit records each slot's pinned result copy starts with
@@ -61,7 +62,9 @@ constexpr uint32_t kPreallocHits = 16384;          // hit records each slot's pi
 struct ffbf_server {
     int device = 0;
     int num_sms = 0;
-    cudaStream_t st_scan = nullptr, st_copy = nullptr;
+    // request copies: texts of kSmallCopy bytes or less on st_copy_small, so that they do not queue behind
+    // large texts on st_copy (the two copies share the link while both run)
+    cudaStream_t st_scan = nullptr, st_copy = nullptr, st_copy_small = nullptr;
     Clock::time_point t0;
     std::string err;
 
@@ -188,13 +191,13 @@ void admit(ffbf_server* s) {
         r->off = off;
         r->span = span;
         r->t_admit = s->now();
-        if (r->len && cudaMemcpyAsync(s->d_arena + off, r->h_text, r->len, cudaMemcpyHostToDevice, s->st_copy) !=
-                          cudaSuccess) {
+        cudaStream_t cs = r->len <= kSmallCopy ? s->st_copy_small : s->st_copy;
+        if (r->len && cudaMemcpyAsync(s->d_arena + off, r->h_text, r->len, cudaMemcpyHostToDevice, cs) != cudaSuccess) {
             cudaGetLastError();
             finish(s, r, FFBF_ECUDA);
             continue;
         }
-        cudaEventRecord(s->copy_done[r->slot], s->st_copy);
+        cudaEventRecord(s->copy_done[r->slot], cs);
         s->copying.push_back(r);
     }
 }
@@ -435,6 +438,7 @@ void worker_loop(ffbf_server* s) {
     }
     // stopping: let the device finish what was issued, then drop what is left
     cudaStreamSynchronize(s->st_copy);
+    cudaStreamSynchronize(s->st_copy_small);
     cudaStreamSynchronize(s->st_scan);
     for (auto* c : s->slots) cudaStreamSynchronize(c->st);
     cudaGetLastError();
@@ -458,6 +462,7 @@ void server_free(ffbf_server* s) {
         if (p) cudaFreeHost(p);
     if (s->st_scan) cudaStreamDestroy(s->st_scan);
     if (s->st_copy) cudaStreamDestroy(s->st_copy);
+    if (s->st_copy_small) cudaStreamDestroy(s->st_copy_small);
     auto drop = [](std::deque<Request*>& q) {
         for (auto* r : q) delete r;
         q.clear();
@@ -496,6 +501,7 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
         cudaDeviceGetAttribute(&s->num_sms, cudaDevAttrMultiProcessorCount, device) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->st_scan, cudaStreamNonBlocking) != cudaSuccess ||
         cudaStreamCreateWithFlags(&s->st_copy, cudaStreamNonBlocking) != cudaSuccess ||
+        cudaStreamCreateWithFlags(&s->st_copy_small, cudaStreamNonBlocking) != cudaSuccess ||
         cudaEventCreateWithFlags(&s->batch_done, cudaEventDisableTiming) != cudaSuccess) {
         cudaGetLastError();
         return bail(FFBF_ECUDA);
