@@ -115,3 +115,34 @@ def test_cpp_mirror_header_compiles_and_links(tmp_path):
     (tmp_path / "pats").write_bytes(b"abcdefghijklmnopqrstuvwxyz\n")
     r = subprocess.run([exe, "20", "pats", "out"], input=b"text\n", capture_output=True, cwd=tmp_path)
     assert r.returncode == 1 and b"FilterError" in r.stderr
+
+
+def _bench():
+    import importlib.util
+    spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def test_bench_reads_the_committed_profiles():
+    """bench.py's roofline traffic and probe bound come from the ncu summaries in profiles/."""
+    b = _bench()
+    assert 1.0 < b.profiled_traffic_ratio("scale") < 1.2
+    assert 1.0 < b.profiled_traffic_ratio("plain") < 1.2
+    pb = b.probe_bound("scale", 319.0, 1965.0, 148)
+    assert pb["probes_per_text_byte"] == pytest.approx(0.765)
+    assert pb["achieved"] == pytest.approx(0.765 * 319e9 / (148 * 1965e6))
+    assert b.probe_bound("plain", 500.0, 1965.0, 148) is None  # no probe row for the sparse workload
+    assert b.probe_bound("scale", 319.0, None, 148) is None     # no clock sample, no figure
+
+
+def test_bench_pattern_override_names_its_own_workload(monkeypatch):
+    """--patterns makes another workload: its line names it and no committed profile applies to it."""
+    import sys
+    b = _bench()
+    monkeypatch.setattr(sys, "argv", ["bench.py", "--patterns", "200000", "--text-bytes", str(1 << 20)])
+    wl = b.workload(b.parse())
+    assert wl.name == "scale_200k" and wl.n_patterns == 200000 and wl.text_bytes == 1 << 20
+    assert b.profiled_traffic_ratio(wl.name) is None
+    assert b.describe(wl)["workload"].startswith("scale_200k: 200000 patterns")
