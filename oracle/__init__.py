@@ -20,7 +20,15 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 LIB = os.path.join(HERE, "_build", "libffbf_oracle.so")
 REF_DIR = os.path.join(HERE, "_ref")
-DEFAULT_REF_SRC = "/root/reference"
+REF_ENV = "FFBF_REFERENCE"  # names a checkout of efficient/ffbf; needed only to (re)build oracle/_ref
+
+
+def reference_source():
+    """The efficient/ffbf checkout named by FFBF_REFERENCE, or None when it is unset or not a checkout."""
+    src = os.environ.get(REF_ENV)
+    if src and os.path.exists(os.path.join(src, "src", "rabin-karp", "ffbf.cpp")):
+        return src
+    return None
 
 
 class OParams(ctypes.Structure):
@@ -183,13 +191,12 @@ def ref_name(prm):
 
 
 def ref_binary(prm, ref_src=None, build=True):
-    """Path of the reference binary for this geometry; builds it when the reference sources are present."""
+    """Path of the reference binary for this geometry. A missing (or, with sources at hand, stale) binary is
+    built when `build` is set and the reference sources are given (`ref_src` or FFBF_REFERENCE)."""
     path = os.path.join(REF_DIR, ref_name(prm))
-    if os.path.exists(path):
-        return path
-    src = ref_src or os.environ.get("FFBF_REFERENCE", DEFAULT_REF_SRC)
-    if not build or not os.path.exists(os.path.join(src, "src", "rabin-karp", "ffbf.cpp")):
-        return None
+    src = ref_src or reference_source()
+    if not build or src is None:
+        return path if os.path.exists(path) else None
     subprocess.run(["make", "-s", "-C", HERE, "ref", f"REF={src}", f"LEN={prm.len}", f"K={prm.k}", f"S={prm.s}",
                     f"CACHE={prm.cache_bits:#x}", f"EXT={prm.ext_bits:#x}"], check=True)
     return path

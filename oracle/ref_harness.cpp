@@ -15,6 +15,11 @@
 //  * When FFBF_REF_DUMP names a file, the destructor's munmap first writes the whole mapping there
 //    (main bit array then feed-forward bit array, N/8 bytes each), so tests can compare the
 //    feed-forward filter, which the reference never saves.
+//  * When FFBF_REF_FF_IN names a file of N/8 bytes, the mapping's feed-forward half starts with that
+//    file's contents instead of zeros. Run over an empty stdin, processFile then sets no bit and
+//    filterPhrases (ffbf.cpp:394-485) prunes the patterns with the given feed-forward array: the OR
+//    of the arrays that runs over line-aligned shards of one text dumped, which equals the array a
+//    single run over the whole text builds (a window never spans a '\n').
 #include <errno.h>
 #include <fcntl.h>
 #include <math.h>
@@ -42,7 +47,18 @@ static inline bool operator<(const read_fn&, int) { return false; }
 static const read_fn read_obj = {};
 
 static void* map_fn(void*, size_t len, int prot, int, int, off_t) {
-    return ::mmap(NULL, len, prot, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+    void* p = ::mmap(NULL, len, prot, MAP_PRIVATE | MAP_ANONYMOUS, -1, 0);
+    const char* ff_in = getenv("FFBF_REF_FF_IN");
+    if (p != MAP_FAILED && ff_in && *ff_in) {
+        FILE* f = fopen(ff_in, "rb");
+        const size_t half = len / 2;
+        if (!f || fread((char*)p + half, 1, half, f) != half) {
+            fprintf(stderr, "FFBF_REF_FF_IN: cannot read %zu bytes from %s\n", half, ff_in);
+            exit(3);
+        }
+        fclose(f);
+    }
+    return p;
 }
 
 static int unmap_fn(void* addr, size_t len) {

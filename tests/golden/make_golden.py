@@ -1,7 +1,7 @@
 """Regenerates the golden fixtures in tests/golden/<case>/ by running the reference's own ffbf binary.
 
 For every case in tests/golden/cases.py: build its inputs, compile efficient/ffbf's src/rabin-karp/ffbf.cpp
-for its geometry (oracle/Makefile; needs a checkout of the reference, FFBF_REFERENCE or the default path),
+for its geometry (oracle/Makefile; needs a checkout of the reference named by FFBF_REFERENCE),
 run `ffbf pats out < text` in a scratch directory, and store what it wrote:
 
   meta.json      geometry, input digest, sizes, the reference's stderr timings

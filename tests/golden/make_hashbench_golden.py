@@ -1,7 +1,7 @@
 """Regenerates tests/golden/hashbench/ by running the reference's own hash benchmark.
 
 efficient/ffbf's src/hashes/hashbench.cc, compiled for the scan's hash (oracle/Makefile target
-`hashbench`, which needs a checkout of the reference: FFBF_REFERENCE or the default path), is run as
+`hashbench`, which needs a checkout of the reference named by FFBF_REFERENCE), is run as
 `hashbench -l input.bin` on a seeded input built here, and its stdout is stored:
 
   input.bin.gz   the input: printable lines of random lengths, and the edges of hashbench's fgets loop --
@@ -46,7 +46,9 @@ def build_input(seed=77):
 
 
 def main():
-    ref = os.environ.get("FFBF_REFERENCE", "/root/reference")
+    ref = os.environ.get("FFBF_REFERENCE")
+    if not ref:
+        raise SystemExit("set FFBF_REFERENCE to a checkout of efficient/ffbf")
     subprocess.run(["make", "-s", "-C", os.path.join(ROOT, "oracle"), "hashbench", f"REF={ref}"], check=True)
     binary = os.path.join(ROOT, "oracle", "_ref", "hashbench")
     data = build_input()

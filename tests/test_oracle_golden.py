@@ -80,15 +80,15 @@ def test_oracle_test_line_semantics():
     assert not o.test_line(first[:5] + b"\n" + first[5:])
 
 
-@pytest.mark.skipif(not os.path.exists(os.path.join(os.environ.get("FFBF_REFERENCE", oracle.DEFAULT_REF_SRC),
-                                                    "src", "rabin-karp", "ffbf.cpp")),
-                    reason="reference sources not present")
 @pytest.mark.parametrize("name", ["edge_mixed", "pats_no_newline"])
 def test_fixtures_are_current(name):
     """Re-runs the reference binary and compares with the stored fixture (catches stale goldens)."""
     g = Golden(name)
     prm, pats, text = build_inputs(name)
-    r = oracle.run_reference(oracle.ref_binary(prm), pats, text=text.tobytes())
+    binary = oracle.ref_binary(prm)
+    if binary is None:
+        pytest.skip("reference binary for this geometry not built (oracle/_ref)")
+    r = oracle.run_reference(binary, pats, text=text.tobytes())
     assert g.matches("stdout", r["stdout"]) and g.matches("bloom", r["bloom"])
     assert g.matches("pruned", r["pruned"]) and g.matches("index", r["index"])
 
