@@ -527,11 +527,20 @@ __device__ __forceinline__ uint32_t nl_bytes(uint32_t w) {
     return ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
 }
 
-// Last '\n' in [lo, p] (p >= lo), or -1: aligned 16-byte chunks from p down to lo.
-__device__ __forceinline__ long long last_nl_back(const uint8_t* text, long long lo, long long p) {
+// The aligned 16 bytes of `text` at c (c a multiple of 16, c < n). The last, partial chunk of a text whose
+// length is not a multiple of 16 is read byte by byte, zero-filled past n, so nothing beyond the text is read.
+__device__ __forceinline__ uint4 chunk16(const uint8_t* text, long long c, long long n) {
+    if (c + 16 <= n) return __ldg(reinterpret_cast<const uint4*>(text + c));
+    uint32_t w[4] = {0u, 0u, 0u, 0u};
+    for (int i = 0; i < 16 && c + i < n; i++) w[i >> 2] |= (uint32_t)__ldg(text + c + i) << (8 * (i & 3));
+    return make_uint4(w[0], w[1], w[2], w[3]);
+}
+
+// Last '\n' in [lo, p] (lo <= p < n), or -1: aligned 16-byte chunks from p down to lo.
+__device__ __forceinline__ long long last_nl_back(const uint8_t* text, long long n, long long lo, long long p) {
     while (p >= lo) {
         const long long c = p & ~15LL;
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(text + c));
+        const uint4 v = chunk16(text, c, n);
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
         // bytes of the chunk at offsets max(lo - c, 0) .. p - c
         const int hi = (int)(p - c), low = (int)max(lo - c, 0LL);
@@ -547,11 +556,11 @@ __device__ __forceinline__ long long last_nl_back(const uint8_t* text, long long
     return -1;
 }
 
-// First '\n' in [q, hi) (q < hi), or -1: aligned 16-byte chunks from q up to hi.
-__device__ __forceinline__ long long first_nl_fwd(const uint8_t* text, long long q, long long hi) {
+// First '\n' in [q, hi) (q < hi <= n), or -1: aligned 16-byte chunks from q up to hi.
+__device__ __forceinline__ long long first_nl_fwd(const uint8_t* text, long long n, long long q, long long hi) {
     while (q < hi) {
         const long long c = q & ~15LL;
-        const uint4 v = __ldg(reinterpret_cast<const uint4*>(text + c));
+        const uint4 v = chunk16(text, c, n);
         const uint32_t w[4] = {v.x, v.y, v.z, v.w};
         const int low = (int)(q - c), top = (int)min(hi - c, 16LL) - 1;  // offsets low .. top
         for (int k = low >> 2; k <= (top >> 2); k++) {
@@ -574,7 +583,7 @@ __global__ void k_resolve(const uint8_t* text, uint64_t n, uint32_t len, const H
     uint64_t s = 0;
     if (w > 0) {
         const uint64_t tb = (w - 1) / kScanTile;
-        const long long p = last_nl_back(text, (long long)(tb * kScanTile), (long long)w - 1);
+        const long long p = last_nl_back(text, (long long)n, (long long)(tb * kScanTile), (long long)w - 1);
         s = p >= 0 ? (uint64_t)p + 1 : (uint64_t)(prev_nl[tb] + 1);
     }
     // line end: the first '\n' after the window in its tile, else the suffix summary, else the text's end
@@ -583,7 +592,7 @@ __global__ void k_resolve(const uint8_t* text, uint64_t n, uint32_t len, const H
     if (q < n) {
         const uint64_t te = q / kScanTile;
         const uint64_t hi = min(n, (te + 1) * (uint64_t)kScanTile);
-        const long long f = first_nl_fwd(text, (long long)q, (long long)hi);
+        const long long f = first_nl_fwd(text, (long long)n, (long long)q, (long long)hi);
         if (f >= 0) e = (uint64_t)f;
         else e = next_nl[te] == LLONG_MAX ? n : (uint64_t)next_nl[te];
     }

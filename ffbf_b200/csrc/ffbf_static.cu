@@ -9,10 +9,10 @@
 // the outputs (feed-forward filter, hit and line arrays) in device memory it owns.
 //
 // The array lives in every GPU that loads this library until the process exits. Its device address is
-// looked up once per device, on the first call made with that device current.
+// looked up on every call, in the context current at the call (a lookup allocates nothing), so a
+// cudaDeviceReset between calls, or a driver-API context of the caller's own, gets the array of the
+// context it runs in. The first call on a device loads the module that holds the array there.
 #include <cuda_runtime.h>
-
-#include <mutex>
 
 #include "../../include/ffbf.h"
 #include "ffbf_kernels.cuh"
@@ -35,28 +35,17 @@ static_assert(kScratchBytes == FFBF_STATIC_SCRATCH_BYTES, "scratch size in inclu
 // cudaGetSymbolAddress returns for the current device, never &g_scan_scratch.
 static __device__ __align__(256) unsigned char g_scan_scratch[kScratchBytes];
 
-constexpr int kMaxDevices = 64;
-std::mutex g_mu;
-unsigned char* g_dev_ptr[kMaxDevices] = {};
-
-// Per-device set-up: the first call made with a device current resolves the array's address there.
-ffbf_status scratch_for_current_device(unsigned char** out) {
-    int dev = -1;
-    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= kMaxDevices) {
+// The array's device address in the current context. Looked up on every call rather than cached: after a
+// cudaDeviceReset the module is loaded again and the array may move, and a caller's own driver-API context
+// on the same device has an array of its own.
+ffbf_status scratch_for_current_context(unsigned char** out) {
+    void* p = nullptr;
+    const cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
+    if (e != cudaSuccess || !p) {
         cudaGetLastError();
         return FFBF_ECUDA;
     }
-    std::lock_guard<std::mutex> lock(g_mu);
-    if (!g_dev_ptr[dev]) {
-        void* p = nullptr;
-        cudaError_t e = cudaGetSymbolAddress(&p, g_scan_scratch);
-        if (e != cudaSuccess || !p) {
-            cudaGetLastError();
-            return FFBF_ECUDA;
-        }
-        g_dev_ptr[dev] = static_cast<unsigned char*>(p);
-    }
-    *out = g_dev_ptr[dev];
+    *out = static_cast<unsigned char*>(p);
     return FFBF_OK;
 }
 
@@ -86,7 +75,7 @@ extern "C" ffbf_status ffbf_scan_static(const ffbf_params* p, const uint32_t* d_
     if (len && (!d_text || ((uintptr_t)d_text & 15))) return FFBF_EINVAL;
     *n_hits = 0;
     unsigned char* scratch = nullptr;
-    ffbf_status s = scratch_for_current_device(&scratch);
+    ffbf_status s = scratch_for_current_context(&scratch);
     if (s != FFBF_OK) return s;
     cudaStream_t st = static_cast<cudaStream_t>(stream);
 

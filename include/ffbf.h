@@ -300,9 +300,13 @@ uint64_t ffbf_kernel_launches(void);
  * return *n_hits holds the number of hit windows; d_hit_offsets[i] is a window start and
  * [d_line_start[i], d_line_end[i]) its line, in no particular order. All scratch memory comes from one
  * fixed device array of FFBF_STATIC_SCRATCH_BYTES compiled into the library, which every GPU that loads
- * the library holds until the process exits. The first call on a device looks up that array's address
- * for the device that is current. Work is ordered on `stream` (a cudaStream_t, 0 for the default);
- * the call waits for it. Calls whose work overlaps on the GPU share the array and race: serialise them.
+ * the library holds until the process exits. Every call looks up that array's address in the context
+ * current at the call (a lookup allocates nothing): after a cudaDeviceReset the next call finds the
+ * reloaded array, and a caller's own driver-API context on the device uses the array of that context.
+ * The first call in a context loads the module that holds the array there; make it before any stream
+ * capture begins in that context. Work is ordered on `stream` (a cudaStream_t, 0 for the default); the
+ * call waits for it. The array keeps the last call's contents (the call clears what must start at zero).
+ * Calls whose work overlaps on the GPU share the array and race: serialise them.
  * Returns FFBF_EINVAL for a text longer than FFBF_STATIC_MAX_TEXT, and FFBF_ENOMEM_DEVICE when more than
  * FFBF_STATIC_MAX_HITS windows hit (*n_hits then holds the full count, the arrays a subset of it). */
 #define FFBF_STATIC_MAX_TEXT (1ull << 30)
