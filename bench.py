@@ -15,9 +15,10 @@ metric through the public C ABI from pinned host memory: ffbf_scan (H2D copy, sc
     python bench.py [--gpus N --steps K --warmup W] [--impl reference] [--workload scale|plain|binary]
 
 With --impl reference the same workload is scanned by efficient/ffbf's own x86 binary (oracle/_ref, built
-from the reference sources) on all host cores: one process per core, each on its own line-aligned shard of
-the text, filter loaded from a __bloom_filter_ cache; throughput = shard bytes / the slowest process's
-`processFile time` (the reference's own timer).
+from the reference sources) on all host cores: the whole text, cut into one line-aligned shard per core, one
+process per shard, filter loaded from a __bloom_filter_ cache; throughput = text bytes / the slowest
+process's `processFile time` (the reference's own timer). A child process writes the inputs, so the arm's
+own process loads none of this repository's native libraries.
 """
 import argparse
 import collections
@@ -57,8 +58,14 @@ def parse():
                     help="override the workload's pattern count (the line then names it, e.g. scale_200k)")
     ap.add_argument("--seed", type=int, default=2024)
     ap.add_argument("--e2e-steps", type=int, default=0, help="steps of the end-to-end leg (default: min(steps, 5))")
-    ap.add_argument("--cpu-sample", type=int, default=1 << 30, help="bytes of text for the CPU baseline")
+    ap.add_argument("--cpu-sample", type=int, default=0,
+                    help="bytes of text for the CPU baseline (default: 1 GiB; the whole 64 MiB plain text; 512 MiB "
+                         "of the binary text; 2 GiB of the batched jobs)")
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-plain", action="store_true", help="skip the plain leg of the default run")
+    ap.add_argument("--no-binary", action="store_true", help="skip the binary leg of the default run")
+    ap.add_argument("--write-reference-inputs", default=None, help=argparse.SUPPRESS)
+    ap.add_argument("--ref-shards", type=int, default=1, help=argparse.SUPPRESS)
     return ap.parse_args()
 
 
@@ -187,125 +194,127 @@ def measured_peaks():
 
 
 # ---- the reference on the host cores ----------------------------------------------------------------
-def line_shards(text, n_shards, shard_bytes):
-    """Line-aligned [a, b) slices: shard i starts after the first '\\n' at or past i*shard_bytes."""
-    out = []
-    for i in range(n_shards):
-        a = i * shard_bytes
-        b = (i + 1) * shard_bytes
-        if b > text.size:
-            break
-        if a > 0:
-            nl = np.flatnonzero(text[a:a + 65536] == 10)
-            a = a + int(nl[0]) + 1 if nl.size else a
-        nl = np.flatnonzero(text[b:b + 65536] == 10)
-        b = b + int(nl[0]) + 1 if nl.size else b
-        out.append((a, min(b, text.size)))
-    return out
-
-
 def reference_binary(prm):
     import oracle
-    return oracle.ref_binary(prm, build=os.path.exists(oracle.DEFAULT_REF_SRC))
+    return oracle.ref_binary(prm)
 
 
-def prepare_reference_dirs(binary, pats, text, shards):
-    """One scratch dir per shard holding pats, the shard text and a __bloom_filter_pats cache built by the
-    reference itself (one run over an empty text)."""
-    base = tempfile.mkdtemp(prefix="ffbf_refbench_", dir="/dev/shm" if os.path.isdir("/dev/shm") else None)
-    seed_dir = os.path.join(base, "seed")
-    os.makedirs(seed_dir)
-    with open(os.path.join(seed_dir, "pats"), "wb") as f:
-        f.write(pats.tobytes())
-    open(os.path.join(seed_dir, "empty"), "wb").close()
-    with open(os.path.join(seed_dir, "empty"), "rb") as fin:
-        subprocess.run([binary, "pats", "out"], stdin=fin, stdout=subprocess.DEVNULL, stderr=subprocess.DEVNULL,
-                       cwd=seed_dir, check=True)
-    dirs = []
-    for i, (a, b) in enumerate(shards):
-        d = os.path.join(base, f"s{i}")
-        os.makedirs(d)
-        os.link(os.path.join(seed_dir, "pats"), os.path.join(d, "pats"))
-        shutil.copyfile(os.path.join(seed_dir, "__bloom_filter_pats"), os.path.join(d, "__bloom_filter_pats"))
-        text[a:b].tofile(os.path.join(d, "text"))
-        dirs.append((d, b - a))
-    return base, dirs
-
-
-def run_reference_step(binary, dirs):
-    procs = []
-    for d, _ in dirs:
-        fin = open(os.path.join(d, "text"), "rb")
-        p = subprocess.Popen([binary, "pats", "out"], stdin=fin, stdout=subprocess.DEVNULL, stderr=subprocess.PIPE,
-                             cwd=d)
-        procs.append((p, fin))
-    times = []
-    for p, fin in procs:
-        _, err = p.communicate()
-        fin.close()
-        if p.returncode != 0:
-            raise RuntimeError(f"reference exited {p.returncode}: {err.decode(errors='replace')}")
-        t = [float(x.split(b":")[1]) for x in err.splitlines() if x.startswith(b"processFile time:")]
-        times.append(t[0])
-    return max(times)
+def host_cores():
+    return len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else (os.cpu_count() or 1)
 
 
 def cpu_baseline_single(wl, pats, text, sample_bytes):
-    """The reference binary on one core over a bounded, line-aligned prefix of the workload text."""
+    """The reference binary on one core over a bounded, line-aligned prefix of the workload text, its filter
+    loaded from a __bloom_filter_ cache it built itself; timed by its own processFile timer."""
+    from oracle.shards import ReferenceShards, line_shards
     binary = reference_binary(wl.params)
     if binary is None:
         return {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                 "sample": "unavailable: reference binary for this geometry was not built"}
-    shards = line_shards(text, 1, min(sample_bytes, text.size - 65536))
-    base, dirs = prepare_reference_dirs(binary, pats, text, shards)
-    try:
-        t = run_reference_step(binary, dirs)
-    finally:
-        shutil.rmtree(base, ignore_errors=True)
-    nbytes = dirs[0][1]
-    return {"value": nbytes / t / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
-            "sample": f"{nbytes / 2**20:.0f} MiB line-aligned prefix of the workload text, 1 process, filter "
-                      f"loaded from its __bloom_filter_ cache; processFile time {t:.3f} s"}
+    cut = line_shards(text, max(1, -(-text.size // max(1, sample_bytes))))[0][1]
+    with ReferenceShards(binary, pats, text, [(0, cut)]) as ref:
+        ref.prepare()
+        t = ref.run(procs=1)[0]
+    return {"value": cut / t / 1e9, "unit": UNIT, "cores": 1, "kind": "reference",
+            "sample": f"{cut / 2**20:.0f} MiB line-aligned prefix of the workload text, 1 process, filter loaded "
+                      f"from its __bloom_filter_ cache; processFile time {t:.3f} s"}
+
+
+def write_reference_inputs(args):
+    """Child process of the reference arm: writes the workload's pattern file and its text, cut into
+    line-aligned shards covering all of it, under args.write_reference_inputs (the arm's own process loads
+    none of this repository's native libraries)."""
+    from oracle.shards import ReferenceShards, line_shards
+    wl = workload(args)
+    pats = wl.patterns(args.seed)
+    text = wl.text(args.seed, pats)
+    shards = line_shards(text, args.ref_shards)
+    ReferenceShards(None, pats, text, shards, base=args.write_reference_inputs).write_shards(
+        write_threads=min(16, host_cores()))
+    return 0
 
 
 def main_reference(args):
+    """efficient/ffbf's own x86 processFile (oracle/_ref) over the whole workload text on all host cores:
+    one process per core, each on a line-aligned shard, all shards together covering the text; one step =
+    every shard scanned once; step time = the slowest process's `processFile time` (the reference's own
+    timer). The inputs are written by a child process."""
     rank = int(os.environ.get("RANK", "0"))
     if rank != 0:
         return 0
+    from oracle.shards import ReferenceShards, scratch_base
     wl = workload(args)
     binary = reference_binary(wl.params)
     cfg = describe(wl)
     if binary is None:
         print(json.dumps({"impl": "reference", "unavailable": "reference binary for this geometry not built"}))
         return 0
-    pats = wl.patterns(args.seed)
-    text = wl.text(args.seed, pats)
-    cores = len(os.sched_getaffinity(0)) if hasattr(os, "sched_getaffinity") else os.cpu_count()
-    nproc = max(1, min(cores, 64))
-    shard = min(32 << 20, (text.size - 65536) // nproc)
-    shards = line_shards(text, nproc, shard)
-    base, dirs = prepare_reference_dirs(binary, pats, text, shards)
+    nproc = max(1, min(host_cores(), 64))
+    base = scratch_base(wl.text_bytes)
     try:
-        total = sum(n for _, n in dirs)
+        cmd = [sys.executable, os.path.abspath(__file__), "--workload", args.workload, "--seed", str(args.seed),
+               "--write-reference-inputs", base, "--ref-shards", str(nproc)]
+        if args.text_bytes:
+            cmd += ["--text-bytes", str(args.text_bytes)]
+        if args.patterns:
+            cmd += ["--patterns", str(args.patterns)]
+        subprocess.run(cmd, check=True, env=dict(os.environ, WORLD_SIZE="1", RANK="0"))
+        ref = ReferenceShards(binary, base=base).build_cache()
+        total = sum(ref.shard_bytes())
         for _ in range(args.warmup):
-            run_reference_step(binary, dirs)
-        ts = [run_reference_step(binary, dirs) for _ in range(args.steps)]
+            ref.run(procs=nproc)
+        ts = [max(ref.run(procs=nproc)) for _ in range(args.steps)]
     finally:
         shutil.rmtree(base, ignore_errors=True)
     t = statistics.mean(ts)
     value = total / t / 1e9
+    n = len(ref.dirs)
     line = {"impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus,
             "steps": args.steps, "warmup": args.warmup, "ms_per_step": t * 1e3, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "u8", "data": "synthetic", "config": cfg,
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": len(dirs), "kind": "reference",
-                             "sample": f"{len(dirs)} processes x {shard / 2**20:.0f} MiB line-aligned shards "
-                                       f"({total / 2**30:.2f} GiB per step), filter from __bloom_filter_ cache"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": n, "kind": "reference",
+                             "sample": f"the whole {total / 2**30:.2f} GiB text in {n} line-aligned shards, one "
+                                       f"process each on {n} host cores; filter from a __bloom_filter_ cache"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
 
 
 # ---- batched form: 512 uneven jobs in one graph launch vs plain per-job launches ------------------------
+def cpu_baseline_jobs(jobs, pats, texts, sample_bytes, seed):
+    """The reference binary over a seeded random sample of the batched jobs, one process per job and as
+    many at a time as there are host cores (each job's filter loaded from the __bloom_filter_ cache its
+    process built beforehand); aggregate = sampled text bytes / wall time of the pool."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle.shards import ReferenceShards, run_many
+    order = np.random.default_rng(seed ^ 0xC0BE).permutation(len(jobs))
+    pick, total = [], 0
+    for j in order:
+        if total >= sample_bytes:
+            break
+        pick.append(int(j))
+        total += jobs[j].text_bytes
+    binaries = {j: reference_binary(jobs[j].params) for j in pick}
+    if any(b is None for b in binaries.values()):
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: a reference binary of the batched geometry menu was not built"}
+    cores = host_cores()
+    refs = [ReferenceShards(binaries[j], pats[j], texts[j], [(0, jobs[j].text_bytes)]) for j in pick]
+    try:
+        with ThreadPoolExecutor(cores) as ex:
+            list(ex.map(lambda r: r.prepare(write_threads=1), refs))
+        wall = run_many(refs, cores)
+    finally:
+        for r in refs:
+            r.close()
+    return {"value": total / wall / 1e9, "unit": UNIT, "cores": min(cores, len(pick)), "kind": "reference",
+            "sample": f"{len(pick)} of the {len(jobs)} jobs picked at random ({total / 2**30:.2f} GiB, "
+                      f"{len({jobs[j].params.cache_bits for j in pick})} of the menu's geometries), one reference "
+                      f"process per job, {cores} at a time; wall time of the pool (process start, filter load "
+                      f"from its cache, processFile, filterPhrases)"}
+
+
 def ff_digest(f):
     """A 64-bit digest of a filter's feed-forward bit array (copied to the host)."""
     import ctypes
@@ -432,6 +441,42 @@ def run_batched(args, local):
         return all(np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1]) and np.array_equal(a[2], c[2])
                    and a[3] == c[3] for a, c in zip(x, y))
 
+    # Ideal schedule: every job scanned at the rate its configuration reaches on the GPU alone (measured on
+    # the largest job of each (configuration, geometry) class), with no launch gaps and perfect packing.
+    # No schedule of these kernels beats it; batched / ideal says how much of the step is packing overhead.
+    def cls(f):
+        t, m = f.config()
+        return (t, m, f.probe_order() if m == 1 else -1, f.params.cache_bits)
+    rates = {}
+    for key in {cls(f) for f in filters}:
+        j = max((i for i, f in enumerate(filters) if cls(f) == key), key=lambda i: jobs[i].text_bytes)
+        f, w, o = filters[j], jobs[j], offs[j]
+        fst = torch.cuda.ExternalStream(f.stream, device=dev)
+        ms = []
+        for _ in range(5):
+            e0.record(fst)
+            f.process_device(base + o, w.text_bytes)
+            e1.record(fst)
+            fst.synchronize()
+            ms.append(e0.elapsed_time(e1))
+        rates[key] = (w.text_bytes / (statistics.median(ms[1:]) * 1e-3), w.text_bytes)
+    ideal_s = sum(w.text_bytes / rates[cls(f)][0] for f, w in zip(filters, jobs))
+    ideal = {"ms": ideal_s * 1e3, "gbs": nbytes / ideal_s / 1e9,
+             "batched_over_ideal": t_batch / ideal_s, "plain_serial_over_ideal": t_plain / ideal_s,
+             "classes": [{"threads": k[0], "mode": k[1], "order": k[2], "cache_bits": k[3],
+                          "jobs": sum(cls(f) == k for f in filters),
+                          "bytes": sum(w.text_bytes for f, w in zip(filters, jobs) if cls(f) == k),
+                          "gbs_alone": r / 1e9, "measured_on_bytes": n} for k, (r, n) in sorted(rates.items())],
+             "how": "sum over jobs of bytes / (its class's rate on the class's largest job, alone on the GPU)"}
+
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_jobs(jobs, pats, [hv[o:o + w.text_bytes] for w, o in zip(jobs, offs)],
+                                    args.cpu_sample or (2 << 30), args.seed)
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
+
     out = {
         "workload": f"batched: {len(jobs)} jobs, {sum(w.n_patterns for w in jobs)} patterns (per job 1k-256k "
                     f"log-uniform, 24-48 B, LEN 24), {nbytes / 2**30:.2f} GiB text (per job 256 KiB-"
@@ -448,9 +493,12 @@ def run_batched(args, local):
         "setup_s": {"generate_and_build": gen_s, "autotune": tune_s, "batch_prepare": prepare_s},
         "autotune_classes": n_classes,
         "configs": dict(collections.Counter(
-            (f"dense-{f.config()[0]}-order{f.probe_order()}" if f.config()[1] else f"sparse-{f.config()[0]}")
+            (f"dense-{f.config()[0]}-order{f.probe_order()}" if f.config()[1] == 1 else
+             f"sparse-deferred-{f.config()[0]}" if f.config()[1] == 2 else f"sparse-{f.config()[0]}")
             for f in filters)),
         "timing": "host clock between device-idle points, median of steps; batched_device = CUDA events",
+        "ideal_schedule": ideal,
+        "cpu_baseline": cpu,
     }
     b.close()
     for f in filters:
@@ -471,6 +519,49 @@ def served_trace(n, rate, seed, n_sets, pool_bytes):
     sizes = np.maximum(sizes, 1)
     offs = (rng.integers(0, pool_bytes - sizes + 1) // 256 * 256).astype(np.int64)
     return [(float(a), int(si), int(o), int(z)) for a, si, o, z in zip(arrivals, sets, offs, sizes)]
+
+
+def cpu_baseline_requests(prm, pats, pool, trace, results, seed, n_sample=256):
+    """The reference binary on a seeded random sample of the served requests (one process per request, as
+    many at a time as there are host cores, each set's filter from a __bloom_filter_ cache built beforehand),
+    and a spot check: each sampled request's lines as the server returned them, printed by processFile's
+    rules, equal what the reference printed for that request's text."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    from oracle.shards import ReferenceShards, run_many
+
+    from ffbf_b200 import format_spans
+    binary = reference_binary(prm)
+    if binary is None:
+        return {"value": None, "unit": UNIT, "cores": 0, "kind": "reference",
+                "sample": "unavailable: reference binary for the served geometry was not built"}
+    pick = np.random.default_rng(seed ^ 0x5A3F).choice(len(trace), size=min(n_sample, len(trace)), replace=False)
+    by_set = collections.defaultdict(list)
+    for i in sorted(int(x) for x in pick):
+        by_set[trace[i][1]].append(i)
+    refs = {si: ReferenceShards(binary, pats[si], pool, [(trace[i][2], trace[i][2] + trace[i][3]) for i in ids])
+            for si, ids in by_set.items()}
+    cores = host_cores()
+    try:
+        with ThreadPoolExecutor(cores) as ex:
+            list(ex.map(lambda r: r.prepare(write_threads=4), refs.values()))
+        wall = run_many(list(refs.values()), cores)
+        mismatches = 0
+        for si, ids in by_set.items():
+            for k, i in enumerate(ids):
+                _, _, o, z = trace[i]
+                r = results[i]
+                mine = format_spans(pool[o:o + z], r.line_start, r.line_end)
+                mismatches += mine != refs[si].stdout(k)
+    finally:
+        for r in refs.values():
+            r.close()
+    nbytes = sum(trace[int(i)][3] for i in pick)
+    return {"value": nbytes / wall / 1e9, "unit": UNIT, "cores": cores, "kind": "reference",
+            "sample": f"{len(pick)} of the {len(trace)} requests picked at random ({nbytes / 2**20:.0f} MiB), one "
+                      f"reference process per request, {cores} at a time; wall time of the pool",
+            "spot_check": {"requests": int(len(pick)), "stdout_equal": int(len(pick) - mismatches),
+                           "against": "the reference binary's stdout for each sampled request's text"}}
 
 
 def wait_until(start, t):
@@ -578,6 +669,12 @@ def run_served(args, local):
 
     srv_res, srv_span, srv_stats, srv_ff = served(True)
     _, sat_span, sat_stats, _ = served(False)
+    cpu = None
+    if not args.no_cpu_baseline:
+        try:
+            cpu = cpu_baseline_requests(prm, pats, pool, trace, srv_res, args.seed)
+        except Exception as e:  # the baseline is reported, never required
+            cpu = {"value": None, "unit": UNIT, "cores": 0, "kind": "reference", "sample": f"failed: {e}"}
     lat = [r.latency for r in srv_res]
     worst = max(range(len(srv_res)), key=lambda i: srv_res[i].latency)
     w = srv_res[worst]
@@ -606,6 +703,7 @@ def run_served(args, local):
                          "gbs": total / plain_span / 1e9, "capacity_gbs": total / plain_cap_span / 1e9},
         "served_over_plain_capacity": plain_cap_span / sat_span,
         "bit_exact_vs_plain": bool(exact),
+        "cpu_baseline": cpu,
         "setup_s": setup_s,
         "timing": "host steady clock; served latency = done - submit inside the server; plain latency = done - "
                   "arrival; every run copies each request's text from pinned host memory",
@@ -753,7 +851,8 @@ def main_ours(args):
     }
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
-            line["cpu_baseline"] = cpu_baseline_single(wl, pats, text, args.cpu_sample)
+            sample = args.cpu_sample or {"binary": 512 << 20}.get(wl.name, 1 << 30)
+            line["cpu_baseline"] = cpu_baseline_single(wl, pats, text, sample)
         except Exception as e:  # the baseline is reported, never required
             line["cpu_baseline"] = {"value": None, "unit": UNIT, "cores": 1, "kind": "reference",
                                     "sample": f"failed: {e}"}
@@ -762,8 +861,10 @@ def main_ours(args):
     torch.cuda.empty_cache()
     rep.close()
     if world == 1 and args.workload == "scale":
-        # the batched and served forms on their own workloads, each in a fresh process on the same GPU
-        for leg, skip in (("batched", args.no_batched), ("served", args.no_served)):
+        # the other workloads (plain, binary) and the batched and served forms, each in a fresh process on the
+        # same GPU
+        for leg, skip in (("plain", args.no_plain), ("binary", args.no_binary), ("batched", args.no_batched),
+                          ("served", args.no_served)):
             if not skip:
                 line[leg] = run_leg(leg, args)
     if rank == 0:
@@ -771,15 +872,24 @@ def main_ours(args):
     return 0
 
 
+LEG_KEYS = ("metric", "value", "unit", "ms_per_step", "config", "roofline", "e2e", "cpu_baseline", "gpu_launches",
+            "clocks", "results")
+
+
 def run_leg(workload, args):
-    """Runs `bench.py --workload <workload>` in a child process and returns its line's summary object."""
+    """Runs `bench.py --workload <workload>` in a child process and returns its line's summary object: the
+    batched/served object, or the headline keys of a plain/binary line."""
     cmd = [sys.executable, os.path.abspath(__file__), "--workload", workload, "--steps", str(args.steps),
            "--warmup", str(args.warmup), "--seed", str(args.seed)]
+    if args.no_cpu_baseline:
+        cmd.append("--no-cpu-baseline")
     p = subprocess.run(cmd, capture_output=True, text=True, env=dict(os.environ, WORLD_SIZE="1", RANK="0"))
     if p.returncode != 0:
         return {"error": f"exit {p.returncode}: {p.stderr.strip().splitlines()[-1] if p.stderr.strip() else ''}"}
     d = json.loads(p.stdout.strip().splitlines()[-1])
-    return dict(d[workload], clocks=d.get("clocks"))
+    if workload in d:
+        return dict(d[workload], clocks=d.get("clocks"))
+    return {k: d[k] for k in LEG_KEYS if k in d}
 
 
 def main_batched(args, rep):
@@ -833,4 +943,6 @@ def main_served(args, rep):
 
 if __name__ == "__main__":
     a = parse()
+    if a.write_reference_inputs:
+        sys.exit(write_reference_inputs(a))
     sys.exit(main_reference(a) if a.impl == "reference" else main_ours(a))

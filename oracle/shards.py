@@ -22,6 +22,7 @@ import os
 import shutil
 import subprocess
 import tempfile
+import time
 from concurrent.futures import ThreadPoolExecutor
 
 import numpy as np
@@ -184,6 +185,16 @@ class ReferenceShards:
 
     def __exit__(self, *exc):
         self.close()
+
+
+def run_many(refs, procs=None):
+    """Scans every shard of several ReferenceShards (their caches built) in one pool of `procs` processes at a
+    time. Returns the pool's wall time in seconds."""
+    jobs = [(r.binary, d) for r in refs for d in r.dirs]
+    t0 = time.perf_counter()
+    with ThreadPoolExecutor(max(1, procs or host_cores())) as ex:
+        list(ex.map(lambda bd: _run(bd[0], bd[1], os.path.join(bd[1], "text")), jobs))
+    return time.perf_counter() - t0
 
 
 def oracle_scan_shards(prm, main, text, shards, threads=None):
