@@ -441,9 +441,10 @@ def run_batched(args, local):
         return all(np.array_equal(a[0], c[0]) and np.array_equal(a[1], c[1]) and np.array_equal(a[2], c[2])
                    and a[3] == c[3] for a, c in zip(x, y))
 
-    # Ideal schedule: every job scanned at the rate its configuration reaches on the GPU alone (measured on
-    # the largest job of each (configuration, geometry) class), with no launch gaps and perfect packing.
-    # No schedule of these kernels beats it; batched / ideal says how much of the step is packing overhead.
+    # Zero-gap schedule of lone jobs: every job scanned at the rate its configuration reaches alone on the GPU
+    # (measured on the largest job of each (configuration, geometry) class), back to back with no launch or
+    # host gaps. plain_serial / it is the share of per-call host and launch overhead in the plain form;
+    # batched / it below 1 means packing jobs together beats even gap-free lone launches.
     def cls(f):
         t, m = f.config()
         return (t, m, f.probe_order() if m == 1 else -1, f.params.cache_bits)
@@ -462,7 +463,7 @@ def run_batched(args, local):
         rates[key] = (w.text_bytes / (statistics.median(ms[1:]) * 1e-3), w.text_bytes)
     ideal_s = sum(w.text_bytes / rates[cls(f)][0] for f, w in zip(filters, jobs))
     ideal = {"ms": ideal_s * 1e3, "gbs": nbytes / ideal_s / 1e9,
-             "batched_over_ideal": t_batch / ideal_s, "plain_serial_over_ideal": t_plain / ideal_s,
+             "batched_over_it": t_batch / ideal_s, "plain_serial_over_it": t_plain / ideal_s,
              "classes": [{"threads": k[0], "mode": k[1], "order": k[2], "cache_bits": k[3],
                           "jobs": sum(cls(f) == k for f in filters),
                           "bytes": sum(w.text_bytes for f, w in zip(filters, jobs) if cls(f) == k),
@@ -497,7 +498,7 @@ def run_batched(args, local):
              f"sparse-deferred-{f.config()[0]}" if f.config()[1] == 2 else f"sparse-{f.config()[0]}")
             for f in filters)),
         "timing": "host clock between device-idle points, median of steps; batched_device = CUDA events",
-        "ideal_schedule": ideal,
+        "lone_jobs_without_gaps": ideal,
         "cpu_baseline": cpu,
     }
     b.close()

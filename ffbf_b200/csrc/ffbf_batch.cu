@@ -88,7 +88,7 @@ ffbf_status build_plan(const std::vector<PlanJob>& jobs, int num_sms, ScanPlan& 
                 Group* gp = nullptr;
                 for (auto& g : groups)
                     if (g.len == c->g.len && g.cfg.mode == cfg.mode && ffbf::config_threads(g.cfg) == threads &&
-                        (cfg.mode == 0 || g.cfg.order == cfg.order))
+                        (cfg.mode != 1 || g.cfg.order == cfg.order))
                         gp = &g;
                 if (!gp) {
                     groups.push_back(Group{c->g.len, cfg, {}});
@@ -417,9 +417,10 @@ ffbf_status autotune_impl(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
     uint32_t* saved = nullptr;
     TRY(dalloc_t(c, &saved, c->filter_bytes / 4));
     CUDA_TRY(c, cudaMemcpyAsync(saved, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
-    // shared-memory mode at three CTA sizes, dense mode at two (its probe order follows the filter's fills)
-    const ffbf::FastConfig cands[] = {{512, 0, 0, 0}, {384, 0, 0, 0}, {256, 0, 0, 0}, {384, 1, 0, 0},
-                                      {256, 1, 0, 0}};
+    // shared-memory mode at three CTA sizes with candidates queued per byte and at two with candidates
+    // deferred to the end of each block, dense mode at two (its probe order follows the filter's fills)
+    const ffbf::FastConfig cands[] = {{512, 0, 0, 0}, {384, 0, 0, 0}, {256, 0, 0, 0}, {256, 2, 0, 0},
+                                      {192, 2, 0, 0}, {384, 1, 0, 0}, {256, 1, 0, 0}};
     ffbf::FastConfig best = c->cfg;
     double best_score = 1e300;
     cudaEvent_t e0, e1;

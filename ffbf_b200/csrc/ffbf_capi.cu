@@ -194,7 +194,7 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
     if (c->borrowed) return FFBF_OK;  // the filter's owner built the table and chose the configuration
     if (c->stage1_dirty || !c->d_stage1) {
         // measured on the sparse table of the configured CTA size (512 while the mode is open)
-        const int tm = c->cfg.mode == 0 ? ffbf::config_threads(c->cfg) : 512;
+        const int tm = c->cfg.mode != 1 ? ffbf::config_threads(c->cfg) : 512;
         TRY(ensure_stage1(c, tm, false, true));
         CUDA_TRY(c, ffbf::popcount_words(c->d_stage1, c->stage1_words, c->d_popc, c->st));
         const uint32_t cw = c->g.cache_bits / 32, ew = (uint32_t)(((uint64_t)c->g.ext_mask + 1) / 32);
@@ -209,18 +209,18 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
             c->cfg.mode = c->force_mode >= 0 ? c->force_mode : c->stage1_fill > 0.3 ? 1 : 0;
             // default CTA sizes (measured best on the 10k- and 1M-pattern workloads): 512 threads for the
             // shared-memory stage, 384 for dense filters
-            c->cfg.threads = c->threads_env ? c->threads_env : c->cfg.mode != 0 ? 384 : 512;
+            c->cfg.threads = c->threads_env ? c->threads_env : c->cfg.mode == 1 ? 384 : c->cfg.mode == 2 ? 256 : 512;
         }
         c->stage1_dirty = false;
     }
     if (c->force_mode >= 0) c->cfg.mode = c->force_mode;
     // the dense mode pipelines two probes of distinct index functions: with K = 1 only the sparse mode applies
-    if (c->g.k < 2) c->cfg.mode = 0;
+    if (c->g.k < 2 && c->cfg.mode == 1) c->cfg.mode = 0;
     // the dense mode's probe order is the filter's, unless the environment fixes it
     c->cfg.order = c->force_order >= 0 ? c->force_order : c->probe_order;
     if (c->g.k < 4 && c->cfg.order == 1) c->cfg.order = 0;  // order 1 probes f2 and f3 first
     // the table the configured kernel reads (a dense kernel without prefilter reads none)
-    if (c->cfg.mode == 0) TRY(ensure_stage1(c, ffbf::config_threads(c->cfg), false, false));
+    if (c->cfg.mode != 1) TRY(ensure_stage1(c, ffbf::config_threads(c->cfg), false, false));
     else if (c->cfg.order == 2) TRY(ensure_stage1(c, ffbf::config_threads(c->cfg), true, false));
     return FFBF_OK;
 }
@@ -382,9 +382,10 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
         return bail(FFBF_ECUDA);
     }
     const char* th = getenv("FFBF_SCAN_THREADS");
-    if (th && (atoi(th) == 256 || atoi(th) == 384 || atoi(th) == 512)) c->cfg.threads = c->threads_env = atoi(th);
+    if (th && (atoi(th) == 192 || atoi(th) == 256 || atoi(th) == 384 || atoi(th) == 512))
+        c->cfg.threads = c->threads_env = atoi(th);
     const char* fm = getenv("FFBF_SCAN_MODE");
-    if (fm && (fm[0] == '0' || fm[0] == '1')) c->force_mode = fm[0] - '0';
+    if (fm && fm[0] >= '0' && fm[0] <= '2') c->force_mode = fm[0] - '0';
     const char* fo = getenv("FFBF_SCAN_ORDER");
     if (fo && fo[0] >= '0' && fo[0] <= '2') c->force_order = fo[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");

@@ -33,6 +33,7 @@
 #include <algorithm>
 #include <climits>
 #include <cmath>
+#include <cstdlib>
 #include <cstring>
 
 #include "ffbf_scan_fast.cuh"
@@ -76,6 +77,22 @@ __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map
         "[%5];" ::"r"(dst),
         "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar)
         : "memory");
+}
+
+// The same load with an L2 cache policy (createpolicy): the text streams through L2 once.
+__device__ __forceinline__ void tma_load_3d_hint(uint32_t dst, const CUtensorMap* map, int x, int y, int z,
+                                                 uint32_t bar, uint64_t policy) {
+    asm volatile(
+        "cp.async.bulk.tensor.3d.shared::cluster.global.tile.mbarrier::complete_tx::bytes.L2::cache_hint "
+        "[%0], [%1, {%2, %3, %4}], [%5], %6;" ::"r"(dst),
+        "l"(map), "r"(x), "r"(y), "r"(z), "r"(bar), "l"(policy)
+        : "memory");
+}
+
+__device__ __forceinline__ uint64_t l2_evict_first_policy() {
+    uint64_t p;
+    asm volatile("createpolicy.fractional.L2::evict_first.b64 %0, 1.0;" : "=l"(p));
+    return p;
 }
 
 // Shared-memory loads the compiler may schedule freely (the tables are read-only after set-up, and every
@@ -206,6 +223,66 @@ __device__ __noinline__ void flush_queue(const FastJob* J, uint32_t qaddr, int q
 // MODE 3: MODE 1 with a shared-memory prefilter: the f0 load is issued only for windows whose bit in the
 // folded cache region (the stage-1 table, sized for the room this kernel leaves) is set, so filters whose
 // fold still rejects many windows issue that many fewer L2 probes.
+// MODE 4 (sparse filters, deferred): MODE 0's two shared-memory probes, but the byte loop only shifts each
+// window's pass bit into a 32-bit register mask; it carries no newline test and no warp vote, so a 32-byte
+// block is one branch-free stretch of code. After the block, the block's newline mask (SWAR) gives each
+// window's validity, and only when a lane of the warp holds a valid passing window is the hash of its 8-byte
+// segment recomputed from a checkpoint, this time queueing the candidates as MODE 0 does. It pays where the
+// stage-1 table rejects nearly every window (a large table: fewer threads per CTA).
+template <int N>
+__device__ __forceinline__ void shl64_or(uint32_t& lo, uint32_t& hi) {
+    // (hi:lo) |= (hi:lo) << N, 0 < N < 32
+    hi |= __funnelshift_l(lo, hi, N);
+    lo |= lo << N;
+}
+
+// Bit j set when the window of L bytes ending at byte j of a 32-byte block holds a '\n'. `prev` and `cur`
+// are the newline masks (bit i = byte i is '\n') of the previous block and of this one.
+template <int L>
+__device__ __forceinline__ uint32_t window_has_newline(uint32_t prev, uint32_t cur) {
+    static_assert(L >= 1 && L <= 32, "windows reach back at most one block");
+    // OR of (cur:prev) << k for k in [0, L), high word: (cur:prev) << k covers [0, w) after the doubling
+    // steps below; the set bits of L add shifted copies of it
+    uint32_t lo = prev, hi = cur;
+    uint32_t rhi = 0;
+    int covered = 0;
+#pragma unroll
+    for (int m = 0; m < 6; m++) {
+        const int w = 1 << m;
+        if (L & w) {
+            if (covered == 0) rhi |= hi;
+            else if (covered < 32) rhi |= __funnelshift_l(lo, hi, covered);
+            else rhi |= lo << (covered - 32);
+            covered += w;
+        }
+        if (2 * w <= L) {
+            switch (w) {
+                case 1: shl64_or<1>(lo, hi); break;
+                case 2: shl64_or<2>(lo, hi); break;
+                case 4: shl64_or<4>(lo, hi); break;
+                case 8: shl64_or<8>(lo, hi); break;
+                case 16: shl64_or<16>(lo, hi); break;
+                default: break;
+            }
+        }
+    }
+    return rhi;
+}
+
+// Newline mask of 4 text bytes: bit k set when byte k of w is '\n' (exact per byte).
+__device__ __forceinline__ uint32_t newline_bits4(uint32_t w) {
+    const uint32_t t = w ^ 0x0A0A0A0Au;
+    const uint32_t zb = ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
+    return (zb * 0x00204081u) >> 28;  // bits 7, 15, 23, 31 -> 28..31, without carries
+}
+
+__device__ __forceinline__ uint32_t newline_mask32(const uint32_t (&w)[8]) {
+    uint32_t m = 0;
+#pragma unroll
+    for (int q = 0; q < 8; q++) m |= newline_bits4(w[q]) << (4 * q);
+    return m;
+}
+
 template <int L, int THREADS, int MODE>
 __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
                                                           uint32_t n_items, uint32_t max_s1_words,
@@ -213,12 +290,13 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
     // ctl[0]: error flags; ctl[1]: the work queue, the count of items handed out past the first wave
     uint32_t* const error_flag = ctl;
     constexpr int kStageBytes = THREADS * kRowBytes;
-    constexpr int kQCap = MODE == 0 ? kQueueCap : 2 * kQueueCap;
+    constexpr int kQCap = (MODE == 0 || MODE == 4) ? kQueueCap : 2 * kQueueCap;
     constexpr int kQBytes = kQCap * 16;
     // dense mode: ring depth per stage (divides 32); 384-thread CTAs trade depth for warps (more L2 probes
     // in flight per SM within the register file)
     constexpr int kRing = THREADS >= 384 ? 4 : 8;
     constexpr int kBox = THREADS > 256 ? THREADS / 2 : THREADS;  // streams per TMA box (<= 256)
+    constexpr bool kTable = MODE == 0 || MODE == 3 || MODE == 4;  // reads the stage-1 table
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -270,8 +348,14 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
         m[2] = nr;
         m[3] = 1;
         mbar_expect_tx(bar, kStageBytes);
-        for (int b = 0; b < THREADS / kBox; b++)
-            tma_load_3d(dst + b * kBox * kRowBytes, &J->tmap, 0, y, z + b * kBox, bar);
+        if (__ldg(&J->text_evict_first)) {
+            const uint64_t pol = l2_evict_first_policy();
+            for (int b = 0; b < THREADS / kBox; b++)
+                tma_load_3d_hint(dst + b * kBox * kRowBytes, &J->tmap, 0, y, z + b * kBox, bar, pol);
+        } else {
+            for (int b = 0; b < THREADS / kBox; b++)
+                tma_load_3d(dst + b * kBox * kRowBytes, &J->tmap, 0, y, z + b * kBox, bar);
+        }
         if (++nr == (int)R) {
             nr = -1;
             ni = gridDim.x + atomicAdd(ctl + 1, 1u);  // next item from the queue
@@ -287,6 +371,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
         s_nr = -1;
         mbar_init(bar0, 1);
         mbar_init(bar1, 1);
+        *reinterpret_cast<uint32_t*>(smem + (bar0 - base) + 64) = 0xFFFFFFFFu;  // MODE 4's one-probe word
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         // publication gate: a bounded poll, and no load in flight if it gives up
         bool open = true;
@@ -345,7 +430,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
     };
     // dense-mode rings. Stage A: the first probe's word (0 when the window was not valid, so its test fails),
     // h1, h2. Stage B: the second probe's word (0 when stage A failed), h1, h2.
-    constexpr int kR = MODE != 0 ? kRing : 1;
+    constexpr int kR = (MODE == 1 || MODE == 2 || MODE == 3) ? kRing : 1;
     // dense mode: rotation of h1/h2 giving the pipelined probes' index functions, and the first probe a
     // queued window still needs in the reference order (MODE 1 knows f0 and f1; MODE 2 retests all)
     constexpr int kRot = MODE == 2 ? 16 : 0;
@@ -357,6 +442,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
     uint32_t hl = 0, hh = 0;
     int lnp = -1000;  // last '\n' relative to the current row start
     uint32_t prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
+    // MODE 4: newline mask of the previous block (bit 31 forced at the text's start, where nothing precedes
+    // offset 0), and the second probe's table (the stage-1 table, or with S = 1 a word of ones: one probe)
+    uint32_t nl_prev = 0;
+    uint32_t s2 = s1, s2_bmask = 0;
 
     for (uint32_t k = 0;; k++) {
         const int* m = meta + 4 * (k & 1);
@@ -391,7 +480,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             R = J->rows;
             spt_log2 = J->streams_per_tile_log2;
             main_words = J->main_words;
-            s1_fits = (MODE != 0 && MODE != 3) || J->stage1_nwords <= max_s1_words;
+            s1_fits = !kTable || J->stage1_nwords <= max_s1_words;
             const uint32_t cmask = g.cache_mask;
             two = g.s > 1;
             one_probe = two ? 0u : 1u;
@@ -404,7 +493,9 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
             b_add = J->b_add;
             // sparse mode: the stage-1 probes are exact when the table is the cache region itself
             s1_first = J->stage1_shift == 0 ? (two ? 2u : 1u) : 0u;
-            if constexpr (MODE == 0 || MODE == 3) {
+            s2 = two ? s1 : bar0 + 64;
+            s2_bmask = two ? s1_bmask : 0u;
+            if constexpr (kTable) {
                 const uint32_t nw = s1_fits ? J->stage1_nwords : 0u;
                 const uint32_t* src = J->stage1_words;
                 for (uint32_t i = tid; i < nw; i += THREADS) s1p[i] = src[i];
@@ -452,6 +543,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                 if (c == 0x0Au) lnp = j - 32;
             }
             if (z == 0) lnp = -1;  // text start: nothing before offset 0
+            if constexpr (MODE == 4) nl_prev = newline_mask32(prev) | (z == 0 ? 0x80000000u : 0u);
             s_fnl[tid] = LLONG_MAX;
             s_lnl[tid] = -1;
         } else {
@@ -474,58 +566,120 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                     cur[4] = v1.x; cur[5] = v1.y; cur[6] = v1.z; cur[7] = v1.w;
                 }
                 const int lnp_blk = lnp;
+                if constexpr (MODE == 4) {
+                    // pass bits of the block's windows (bit j: the window ending at byte j passed both table
+                    // probes), and the hash before each 8-byte segment
+                    uint32_t pass = 0, ckl[4], ckh[4];
 #pragma unroll
-                for (int j = 0; j < 32; j++) {
-                    const uint32_t c = byte_at(cur[j >> 2], j & 3);
-                    uint32_t co;
-                    if (j >= L) co = byte_at(cur[(j - L) >> 2], (j - L) & 3);
-                    else co = byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
-                    const uint2 sv = lds64(lane_tab + c * 128u);
-                    const uint2 o = lds64(lane_tab + co * 128u);
-                    uint32_t rl, rh;
-                    rol_pair<L>(o.x, o.y, rl, rh);
-                    const uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
-                    hl = nl ^ sv.x ^ rl;
-                    hh = nh ^ sv.y ^ rh;
-                    if (c == 0x0Au) lnp = j;
-                    if constexpr (MODE == 0) {
-                        const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
-                        const uint32_t w1 = lds32(s1 + ((hh >> 3) & s1_bmask));
-                        // both table bits in one test (the second is forced on when S = 1)
-                        const uint32_t t = __funnelshift_r(w0, w0, hl) & (__funnelshift_r(w1, w1, hh) | one_probe);
-                        const bool pass = (j - lnp >= L) && (t & 1u) != 0;
-                        enqueue(pass, (uint32_t)(kRowBytes + 32 * b + j), hl, hh, s1_first);
-                    } else {
-                        const int slot = j % kRing;
-                        // stage B: the window that entered stage A 2*kRing bytes ago (a probe's bit sits at
-                        // f & 31 in its word: region offsets are multiples of 32)
-                        const uint32_t fb_old = rot_const<kRot>(ring2_h[slot]);
-                        const bool pass2 = (__funnelshift_r(ring2_v[slot], ring2_v[slot], fb_old) & 1u) != 0;
-                        enqueue(pass2, (uint32_t)(kRowBytes + 32 * b + j - 2 * kRing), ring2_l[slot], ring2_h[slot],
-                                kFirstB);
-                        // stage A: the window issued kRing bytes ago; its word has arrived by now
-                        const uint32_t fa_old = rot_const<kRot>(ring_l[slot]);
-                        const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], fa_old) & 1u) != 0;
-                        ring2_l[slot] = ring_l[slot];
-                        ring2_h[slot] = ring_h[slot];
-                        const uint32_t fb = rot_const<kRot>(ring_h[slot]);
-                        ring2_v[slot] = ldg_if(main_words + (((fb & b_mask) + b_add) >> 5), pass1);
-                        bool issue = j - lnp >= L;
-                        if constexpr (MODE == 3) {
-                            // the folded table's bit: clear means the cache bit of f0 is clear too
-                            const uint32_t w = lds32(s1 + ((hl >> 3) & s1_bmask));
-                            issue = issue && (__funnelshift_r(w, w, hl) & 1u) != 0;
+                    for (int j = 0; j < 32; j++) {
+                        if ((j & 7) == 0) {
+                            ckl[j >> 3] = hl;
+                            ckh[j >> 3] = hh;
                         }
-                        ring_l[slot] = hl;
-                        ring_h[slot] = hh;
-                        const uint32_t fa = rot_const<kRot>(hl);
-                        if constexpr (MODE != 2)  // f0 is in the cache region (S >= 1): no offset
-                            ring_v[slot] = ldg_if(main_words + ((fa & a_mask) >> 5), issue);
-                        else
-                            ring_v[slot] = ldg_if(main_words + (((fa & a_mask) + a_add) >> 5), issue);
+                        const uint32_t c = byte_at(cur[j >> 2], j & 3);
+                        uint32_t co;
+                        if (j >= L) co = byte_at(cur[(j - L) >> 2], (j - L) & 3);
+                        else co = byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
+                        const uint2 sv = lds64(lane_tab + c * 128u);
+                        const uint2 o = lds64(lane_tab + co * 128u);
+                        uint32_t rl, rh;
+                        rol_pair<L>(o.x, o.y, rl, rh);
+                        const uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
+                        hl = nl ^ sv.x ^ rl;
+                        hh = nh ^ sv.y ^ rh;
+                        const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
+                        const uint32_t w1 = lds32(s2 + ((hh >> 3) & s2_bmask));
+                        const uint32_t t = __funnelshift_r(w0, w0, hl) & __funnelshift_r(w1, w1, hh);
+                        pass = __funnelshift_r(pass, t, 1);  // t's bit 0 enters at bit 31
+                    }
+                    const uint32_t nlm = newline_mask32(cur);
+                    if (__any_sync(0xffffffffu, pass != 0u)) {
+                        // valid windows hold no '\n' (processFile resets the hash there); a stream past the
+                        // job's end has none
+                        const uint32_t cand = active ? pass & ~window_has_newline<L>(nl_prev, nlm) : 0u;
+#pragma unroll
+                        for (int sg = 0; sg < 4; sg++) {
+                            if (__any_sync(0xffffffffu, ((cand >> (8 * sg)) & 0xFFu) != 0u)) {
+                                uint32_t ql = ckl[sg], qh = ckh[sg];
+#pragma unroll
+                                for (int jj = 0; jj < 8; jj++) {
+                                    const int j = 8 * sg + jj;
+                                    const uint32_t c = byte_at(cur[j >> 2], j & 3);
+                                    uint32_t co;
+                                    if (j >= L) co = byte_at(cur[(j - L) >> 2], (j - L) & 3);
+                                    else co = byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
+                                    const uint2 sv = lds64(lane_tab + c * 128u);
+                                    const uint2 o = lds64(lane_tab + co * 128u);
+                                    uint32_t rl, rh;
+                                    rol_pair<L>(o.x, o.y, rl, rh);
+                                    const uint32_t nl = __funnelshift_l(qh, ql, 1), nh = __funnelshift_l(ql, qh, 1);
+                                    ql = nl ^ sv.x ^ rl;
+                                    qh = nh ^ sv.y ^ rh;
+                                    enqueue(((cand >> j) & 1u) != 0u, (uint32_t)(kRowBytes + 32 * b + j), ql, qh,
+                                            s1_first);
+                                }
+                            }
+                        }
+                    }
+                    nl_prev = nlm;
+                    if (nlm) {
+                        lnp = 31 - __clz(nlm);
+                        if (row_first < 0 && need_first) row_first = 32 * b + __ffs(nlm) - 1;
+                    }
+                } else {
+#pragma unroll
+                    for (int j = 0; j < 32; j++) {
+                        const uint32_t c = byte_at(cur[j >> 2], j & 3);
+                        uint32_t co;
+                        if (j >= L) co = byte_at(cur[(j - L) >> 2], (j - L) & 3);
+                        else co = byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
+                        const uint2 sv = lds64(lane_tab + c * 128u);
+                        const uint2 o = lds64(lane_tab + co * 128u);
+                        uint32_t rl, rh;
+                        rol_pair<L>(o.x, o.y, rl, rh);
+                        const uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
+                        hl = nl ^ sv.x ^ rl;
+                        hh = nh ^ sv.y ^ rh;
+                        if (c == 0x0Au) lnp = j;
+                        if constexpr (MODE == 0) {
+                            const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
+                            const uint32_t w1 = lds32(s1 + ((hh >> 3) & s1_bmask));
+                            // both table bits in one test (the second is forced on when S = 1)
+                            const uint32_t t = __funnelshift_r(w0, w0, hl) & (__funnelshift_r(w1, w1, hh) | one_probe);
+                            const bool pass = (j - lnp >= L) && (t & 1u) != 0;
+                            enqueue(pass, (uint32_t)(kRowBytes + 32 * b + j), hl, hh, s1_first);
+                        } else {
+                            const int slot = j % kRing;
+                            // stage B: the window that entered stage A 2*kRing bytes ago (a probe's bit sits at
+                            // f & 31 in its word: region offsets are multiples of 32)
+                            const uint32_t fb_old = rot_const<kRot>(ring2_h[slot]);
+                            const bool pass2 = (__funnelshift_r(ring2_v[slot], ring2_v[slot], fb_old) & 1u) != 0;
+                            enqueue(pass2, (uint32_t)(kRowBytes + 32 * b + j - 2 * kRing), ring2_l[slot], ring2_h[slot],
+                                    kFirstB);
+                            // stage A: the window issued kRing bytes ago; its word has arrived by now
+                            const uint32_t fa_old = rot_const<kRot>(ring_l[slot]);
+                            const bool pass1 = (__funnelshift_r(ring_v[slot], ring_v[slot], fa_old) & 1u) != 0;
+                            ring2_l[slot] = ring_l[slot];
+                            ring2_h[slot] = ring_h[slot];
+                            const uint32_t fb = rot_const<kRot>(ring_h[slot]);
+                            ring2_v[slot] = ldg_if(main_words + (((fb & b_mask) + b_add) >> 5), pass1);
+                            bool issue = j - lnp >= L;
+                            if constexpr (MODE == 3) {
+                                // the folded table's bit: clear means the cache bit of f0 is clear too
+                                const uint32_t w = lds32(s1 + ((hl >> 3) & s1_bmask));
+                                issue = issue && (__funnelshift_r(w, w, hl) & 1u) != 0;
+                            }
+                            ring_l[slot] = hl;
+                            ring_h[slot] = hh;
+                            const uint32_t fa = rot_const<kRot>(hl);
+                            if constexpr (MODE != 2)  // f0 is in the cache region (S >= 1): no offset
+                                ring_v[slot] = ldg_if(main_words + ((fa & a_mask) >> 5), issue);
+                            else
+                                ring_v[slot] = ldg_if(main_words + (((fa & a_mask) + a_add) >> 5), issue);
+                        }
                     }
                 }
-                if (lnp != lnp_blk && row_first < 0 && need_first) {
+                if (MODE != 4 && lnp != lnp_blk && row_first < 0 && need_first) {
                     for (int q = 0; q < 8 && row_first < 0; q++) {
                         const uint32_t t = cur[q] ^ 0x0A0A0A0Au;
                         const uint32_t zb = ~(((t & 0x7F7F7F7Fu) + 0x7F7F7F7Fu) | t) & 0x80808080u;
@@ -536,7 +690,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
 #pragma unroll
                 for (int q = 0; q < 8; q++) prev[q] = cur[q];
             }
-            if constexpr (MODE != 0) {
+            if constexpr (MODE == 1 || MODE == 2 || MODE == 3) {
                 // The rings carry over into the stream's next row (whose bytes follow this row's); at the
                 // stream's end they drain: stage-B slot q holds the window ending at 128 - 2*kRing + q,
                 // stage-A slot q the one at 128 - kRing + q; stage-A survivors go to the queue with only
@@ -608,13 +762,14 @@ constexpr size_t static_smem(int threads) { return 16 * (size_t)threads + 8 * (s
 template <int THREADS, int MODE>
 constexpr size_t fixed_smem() {
     return 1024 + 2 * (size_t)THREADS * kRowBytes + kTabBytes + 128 +
-           (THREADS / 32) * (size_t)(MODE == 0 ? kQueueBytes : 2 * kQueueBytes);
+           (THREADS / 32) * (size_t)(MODE == 0 || MODE == 4 ? kQueueBytes : 2 * kQueueBytes);
 }
 
 template <int L, int THREADS, int MODE>
 cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items, uint32_t max_s1_words,
                        uint32_t* d_ctl, int num_sms, cudaStream_t st) {
-    const size_t smem = fixed_smem<THREADS, MODE>() + (MODE == 0 || MODE == 3 ? 4 * (size_t)max_s1_words : 0);
+    const size_t smem =
+        fixed_smem<THREADS, MODE>() + (MODE == 0 || MODE == 3 || MODE == 4 ? 4 * (size_t)max_s1_words : 0);
     cudaError_t e =
         cudaFuncSetAttribute(k_scan_fast<L, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -639,6 +794,13 @@ cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_
         return cfg.threads == 256 ? launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
                                   : launch_cfg<L, 384, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
     }
+    if (cfg.mode == 2) {  // sparse, deferred candidates: 192, 256 or 384 threads (larger stage-1 tables)
+        switch (cfg.threads) {
+            case 192: return launch_cfg<L, 192, 4>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+            case 384: return launch_cfg<L, 384, 4>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+            default: return launch_cfg<L, 256, 4>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
+        }
+    }
     switch (cfg.threads) {
         case 256: return launch_cfg<L, 256, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
         case 384: return launch_cfg<L, 384, 0>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
@@ -649,6 +811,7 @@ cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_
 size_t fixed_smem_for(int threads, bool dense) {
     if (dense) return threads == 256 ? fixed_smem<256, 1>() : fixed_smem<384, 1>();
     switch (threads) {
+        case 192: return fixed_smem<192, 0>();
         case 256: return fixed_smem<256, 0>();
         case 384: return fixed_smem<384, 0>();
         default: return fixed_smem<512, 0>();
@@ -708,6 +871,7 @@ int dense_probe_order(const Geom& g, double cache_fill, double ext_fill) {
 
 int config_threads(const FastConfig& cfg) {
     if (cfg.mode == 1) return cfg.threads == 256 ? 256 : 384;
+    if (cfg.mode == 2) return cfg.threads == 192 || cfg.threads == 384 ? cfg.threads : 256;
     return cfg.threads == 384 || cfg.threads == 512 ? cfg.threads : 256;
 }
 
@@ -743,13 +907,14 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
     job->ff_words = a.ff_words;
     job->stage1_words = stage1_words;
     // the table the kernel reads: the sparse mode's, or the dense mode's prefilter (order 2)
-    const bool reads_table = cfg.mode == 0 || cfg.order == 2;
-    job->stage1_shift = reads_table ? stage1_shift_for(a.g, threads, cfg.mode != 0) : 0;
+    const bool reads_table = cfg.mode != 1 || cfg.order == 2;
+    job->stage1_shift = reads_table ? stage1_shift_for(a.g, threads, cfg.mode == 1) : 0;
     job->stage1_nwords = reads_table ? (uint32_t)(((uint64_t)a.g.cache_bits >> job->stage1_shift) / 32) : 0;
     {
         // dense mode: regions of the pipelined probes, index functions f0/f1 (order 0) or f2/f3 (order 1,
         // which only K >= 4 filters set)
-        if (cfg.mode != 0 && (a.g.k < 2 || (cfg.order == 1 && a.g.k < 4) || cfg.order < 0 || cfg.order > 2))
+        if (cfg.mode < 0 || cfg.mode > 2 ||
+            (cfg.mode == 1 && (a.g.k < 2 || (cfg.order == 1 && a.g.k < 4) || cfg.order < 0 || cfg.order > 2)))
             *err = cudaErrorInvalidValue;
         const uint32_t fa = cfg.order == 1 ? 2u : 0u, fb = fa + 1;
         job->a_mask = fa < a.g.s ? a.g.cache_mask : a.g.ext_mask;
@@ -763,6 +928,12 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
     job->tile_first_nl = a.tile_first_nl;
     job->tile_last_nl = a.tile_last_nl;
     job->n_tiles = a.ntiles;
+    // FFBF_TEXT_L2=normal keeps the default L2 policy for the text's loads (for comparisons)
+    static const bool evict_first = [] {
+        const char* v = getenv("FFBF_TEXT_L2");
+        return !(v && strcmp(v, "normal") == 0);
+    }();
+    job->text_evict_first = evict_first ? 1u : 0u;
     if (n_streams > 0) {
         const uint32_t box_streams = threads > 256 ? (uint32_t)threads / 2 : (uint32_t)threads;
         cuuint64_t dims[3] = {(cuuint64_t)kRowBytes, (cuuint64_t)rows, (cuuint64_t)n_streams};

@@ -31,6 +31,9 @@ struct alignas(64) FastJob {
     long long* tile_first_nl;
     long long* tile_last_nl;
     uint64_t n_tiles;  // 16 KiB tiles of the text (bounds the newline summary writes)
+    // 1: the text's TMA loads carry an L2 evict-first policy (every text byte is read once, so its lines
+    // should leave L2 before the filter's do); 0: the default policy
+    uint32_t text_evict_first;
     // Optional publication gate of the launch (read from its first job): no load is issued until *ready is
     // non-zero; a gate still closed after ready_spins polls ends the launch with the timeout flag.
     const uint32_t* ready;

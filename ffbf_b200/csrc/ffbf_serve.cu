@@ -1,10 +1,14 @@
 // ffbf_serve.cu -- the scan server (ffbf_server_* in include/ffbf.h): resident pattern sets, admission of
-// requests by free slots and arena room, and continuous batching of the admitted requests.
+// requests by free slots and free device memory, and continuous batching of the admitted requests.
 //
 // One host thread runs the loop. Per iteration it
 //   1. takes new submissions into the FIFO of pending requests;
 //   2. admits pending requests in order while a slot and a range of the text arena are free, and starts
-//      each one's host-to-device copy on the copy stream (an event marks its end);
+//      each one's host-to-device copy on the copy stream (an event marks its end). The arena is a list of
+//      device segments: when no segment has room, a new one is allocated only if the device's free memory
+//      (cudaMemGetInfo, which sees every context's allocations) stays above a reserve afterwards and the
+//      arena stays within its cap; otherwise the request waits, in order, until a finished request frees
+//      room or other contexts free memory. Segments beyond the first are given back when the server idles;
 //   3. moves requests whose copy has finished to the ready list;
 //   4. when the previous launch sequence has finished, launches every ready request as one plan
 //      (build_plan/launch_plan: one tuned launch per (LEN, configuration) group, one generic launch for
@@ -42,7 +46,8 @@ struct Request {
     uint32_t set = 0;
     const uint8_t* h_text = nullptr;
     size_t len = 0;
-    uint64_t off = 0;
+    int seg = -1;       // arena segment holding the text
+    uint64_t off = 0;   // offset in that segment
     uint64_t span = 0;  // arena bytes held
     int slot = -1;
     uint32_t nh = 0;  // hit windows, read back with the batch
@@ -55,6 +60,10 @@ constexpr uint64_t kArenaAlign = 256;
 constexpr uint64_t kSmallCopy = 4ull << 20;  // texts up to this size copy on the small-copy stream
 constexpr uint32_t kMaxCtl = 64;  // control-word groups per plan (one per tuned launch, plus one)
 constexpr uint64_t kPreallocText = 512ull << 20;  // request size the slots' scan buffers start out sized for
+constexpr uint64_t kSegmentBytes = 1ull << 30;    // arena growth step (a larger request gets a segment its size)
+constexpr uint64_t kHbmReserve = 1ull << 30;      // device memory the arena leaves free for others
+constexpr double kGrowRetrySeconds = 1e-3;        // pause between growth attempts that found too little memory
+constexpr double kShrinkIdleSeconds = 0.25;       // idle time after which grown segments are given back
 constexpr uint32_t kPreallocHits = 16384;          // hit records each slot's pinned result copy starts with
 
 }  // namespace
@@ -73,9 +82,17 @@ struct ffbf_server {
     std::vector<cudaEvent_t> copy_done;  // per slot
     std::vector<int> free_slots;
 
-    uint8_t* d_arena = nullptr;
-    uint64_t arena_bytes = 0;
-    std::map<uint64_t, uint64_t> free_ranges;  // offset -> length, coalesced
+    struct Segment {
+        uint8_t* base = nullptr;
+        uint64_t bytes = 0;
+        std::map<uint64_t, uint64_t> free_ranges;  // offset -> length, coalesced
+    };
+    std::vector<Segment> segs;    // segs[0] lives as long as the server
+    uint64_t arena_cap = 0;       // most arena bytes the server holds (0: bounded by free device memory only)
+    uint64_t arena_held = 0;      // bytes of all segments
+    uint64_t device_bytes = 0;    // the device's memory
+    double last_grow_fail = -1.0;
+    double idle_since = -1.0;     // when the loop last found nothing admitted (segments shrink after a while)
 
     // plan tables on the device and their pinned staging
     ffbf::FastJob* d_fast = nullptr;
@@ -134,33 +151,102 @@ ffbf_status sfail(ffbf_server* s, ffbf_status st, const std::string& msg) {
     return st;
 }
 
-bool arena_alloc(ffbf_server* s, uint64_t bytes, uint64_t* off) {
-    for (auto it = s->free_ranges.begin(); it != s->free_ranges.end(); ++it) {
+bool seg_alloc(ffbf_server::Segment& g, uint64_t bytes, uint64_t* off) {
+    for (auto it = g.free_ranges.begin(); it != g.free_ranges.end(); ++it) {
         if (it->second >= bytes) {
             *off = it->first;
             const uint64_t rest = it->second - bytes;
             const uint64_t at = it->first + bytes;
-            s->free_ranges.erase(it);
-            if (rest) s->free_ranges[at] = rest;
+            g.free_ranges.erase(it);
+            if (rest) g.free_ranges[at] = rest;
             return true;
         }
     }
     return false;
 }
 
-void arena_free(ffbf_server* s, uint64_t off, uint64_t bytes) {
-    auto it = s->free_ranges.emplace(off, bytes).first;
+void seg_free(ffbf_server::Segment& g, uint64_t off, uint64_t bytes) {
+    auto it = g.free_ranges.emplace(off, bytes).first;
     auto next = std::next(it);
-    if (next != s->free_ranges.end() && it->first + it->second == next->first) {
+    if (next != g.free_ranges.end() && it->first + it->second == next->first) {
         it->second += next->second;
-        s->free_ranges.erase(next);
+        g.free_ranges.erase(next);
     }
-    if (it != s->free_ranges.begin()) {
+    if (it != g.free_ranges.begin()) {
         auto prev = std::prev(it);
         if (prev->first + prev->second == it->first) {
             prev->second += it->second;
-            s->free_ranges.erase(it);
+            g.free_ranges.erase(it);
         }
+    }
+}
+
+// A new segment of at least `bytes`, if the device's free memory stays above the reserve and the arena within
+// its cap. cudaMemGetInfo counts every context's allocations, so memory other processes or libraries took
+// since the last look is respected.
+bool arena_grow(ffbf_server* s, uint64_t bytes) {
+    const double t = s->now();
+    if (s->last_grow_fail >= 0 && t - s->last_grow_fail < kGrowRetrySeconds) return false;
+    uint64_t want = std::max(bytes, kSegmentBytes);
+    if (s->arena_cap) {
+        if (s->arena_held + bytes > s->arena_cap) return false;  // wait for a finished request's room
+        want = std::min(want, s->arena_cap - s->arena_held);
+    }
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess) {
+        cudaGetLastError();
+        s->last_grow_fail = t;
+        return false;
+    }
+    if (free_b < want + kHbmReserve) want = bytes;  // take only what this request needs
+    uint8_t* p = nullptr;
+    if (free_b < want + kHbmReserve || cudaMalloc(&p, want) != cudaSuccess) {
+        cudaGetLastError();
+        s->last_grow_fail = t;
+        return false;
+    }
+    ffbf_server::Segment g;
+    g.base = p;
+    g.bytes = want;
+    g.free_ranges[0] = want;
+    s->segs.push_back(std::move(g));
+    s->arena_held += want;
+    s->last_grow_fail = -1.0;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stats.arena_bytes = s->arena_held;
+    return true;
+}
+
+bool arena_alloc(ffbf_server* s, uint64_t bytes, int* seg, uint64_t* off) {
+    for (size_t i = 0; i < s->segs.size(); i++) {
+        if (seg_alloc(s->segs[i], bytes, off)) {
+            *seg = (int)i;
+            return true;
+        }
+    }
+    if (!arena_grow(s, bytes)) return false;
+    *seg = (int)s->segs.size() - 1;
+    return seg_alloc(s->segs.back(), bytes, off);
+}
+
+void arena_free(ffbf_server* s, int seg, uint64_t off, uint64_t bytes) { seg_free(s->segs[seg], off, bytes); }
+
+// With nothing admitted, the segments grown for earlier requests go back to the device (cudaFree waits for
+// the device, which is idle then).
+void arena_shrink(ffbf_server* s) {
+    bool freed = false;
+    while (s->segs.size() > 1) {
+        auto& g = s->segs.back();
+        if (g.free_ranges.size() != 1 || g.free_ranges.begin()->second != g.bytes) break;
+        cudaFree(g.base);
+        s->arena_held -= g.bytes;
+        s->segs.pop_back();
+        freed = true;
+    }
+    if (freed) {
+        cudaGetLastError();
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stats.arena_bytes = s->arena_held;
     }
 }
 
@@ -169,7 +255,7 @@ void finish(ffbf_server* s, Request* r, ffbf_status st) {
     r->status = st;
     r->t_done = s->now();
     if (r->slot >= 0) s->free_slots.push_back(r->slot);
-    if (r->span) arena_free(s, r->off, r->span);
+    if (r->span) arena_free(s, r->seg, r->off, r->span);
     r->slot = -1;
     r->span = 0;
     std::lock_guard<std::mutex> lk(s->mu);
@@ -184,15 +270,18 @@ void admit(ffbf_server* s) {
         Request* r = s->pending.front();
         const uint64_t span = (r->len + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
         uint64_t off = 0;
-        if (span && !arena_alloc(s, span, &off)) break;  // in order: wait for room
+        int seg = 0;
+        if (span && !arena_alloc(s, span, &seg, &off)) break;  // in order: wait for room
         s->pending.pop_front();
         r->slot = s->free_slots.back();
         s->free_slots.pop_back();
+        r->seg = seg;
         r->off = off;
         r->span = span;
         r->t_admit = s->now();
         cudaStream_t cs = r->len <= kSmallCopy ? s->st_copy_small : s->st_copy;
-        if (r->len && cudaMemcpyAsync(s->d_arena + off, r->h_text, r->len, cudaMemcpyHostToDevice, cs) != cudaSuccess) {
+        if (r->len && cudaMemcpyAsync(s->segs[seg].base + off, r->h_text, r->len, cudaMemcpyHostToDevice, cs) !=
+                          cudaSuccess) {
             cudaGetLastError();
             finish(s, r, FFBF_ECUDA);
             continue;
@@ -227,7 +316,7 @@ void launch_ready(ffbf_server* s) {
     for (Request* r : s->ready) {
         ffbf_ctx* slot = s->slots[r->slot];
         attach_filters(slot, s->sets[r->set]);
-        jobs.push_back({slot, s->d_arena + r->off, r->len});
+        jobs.push_back({slot, s->segs[r->seg].base + r->off, r->len});
         batch.push_back(r);
     }
     s->ready.clear();
@@ -432,9 +521,22 @@ void worker_loop(ffbf_server* s) {
             collect_slow(s);
             progress = true;
         }
+        // With nothing admitted for a while, segments grown for earlier requests go back to the device.
+        const bool quiet = s->copying.empty() && s->ready.empty() && !s->in_flight && s->resolving.empty() &&
+                           s->slow.empty() && s->running.empty();
+        if (quiet && s->pending.empty()) {
+            if (s->idle_since < 0) s->idle_since = s->now();
+            else if (s->segs.size() > 1 && s->now() - s->idle_since > kShrinkIdleSeconds) arena_shrink(s);
+        } else {
+            s->idle_since = -1.0;
+        }
         // Requests on the device or in copies: poll again at once (a sleep rounds up to tens of microseconds
-        // on every stage of a request); with nothing in flight the loop waits on cv_work above.
-        if (!progress) std::this_thread::yield();
+        // on every stage of a request); with nothing in flight the loop waits on cv_work above. Pending requests
+        // that wait for device memory other contexts hold are retried after a pause.
+        if (!progress) {
+            if (quiet && !s->pending.empty()) std::this_thread::sleep_for(std::chrono::microseconds(200));
+            else std::this_thread::yield();
+        }
     }
     // stopping: let the device finish what was issued, then drop what is left
     cudaStreamSynchronize(s->st_copy);
@@ -454,7 +556,9 @@ void server_free(ffbf_server* s) {
         if (h.done) cudaEventDestroy(h.done);
     }
     if (s->batch_done) cudaEventDestroy(s->batch_done);
-    for (void* p : {(void*)s->d_arena, (void*)s->d_fast, (void*)s->d_args, (void*)s->d_counters, (void*)s->d_ctl,
+    for (auto& g : s->segs) cudaFree(g.base);
+    s->segs.clear();
+    for (void* p : {(void*)s->d_fast, (void*)s->d_args, (void*)s->d_counters, (void*)s->d_ctl,
                     (void*)s->d_tail, (void*)s->d_cnt})
         if (p) cudaFree(p);
     for (void* p : {(void*)s->h_fast, (void*)s->h_args, (void*)s->h_counters, (void*)s->h_tail, (void*)s->h_ctl,
@@ -506,15 +610,24 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
         cudaGetLastError();
         return bail(FFBF_ECUDA);
     }
-    if (arena_bytes == 0) arena_bytes = free_b / 2;
-    arena_bytes = arena_bytes / kArenaAlign * kArenaAlign;
-    if (arena_bytes == 0 || arena_bytes > free_b) return bail(FFBF_ENOMEM_DEVICE);
-    if (cudaMalloc(&s->d_arena, arena_bytes) != cudaSuccess) {
-        cudaGetLastError();
-        return bail(FFBF_ENOMEM_DEVICE);
+    // the arena starts as one segment and grows by free device memory up to the cap (0: no cap)
+    s->arena_cap = arena_bytes / kArenaAlign * kArenaAlign;
+    s->device_bytes = total_b;
+    uint64_t first = s->arena_cap ? std::min(s->arena_cap, kSegmentBytes) : kSegmentBytes;
+    if (first + kHbmReserve > free_b)
+        first = free_b > kHbmReserve ? (free_b - kHbmReserve) / kArenaAlign * kArenaAlign : 0;
+    if (first == 0) return bail(FFBF_ENOMEM_DEVICE);
+    {
+        ffbf_server::Segment g;
+        if (cudaMalloc(&g.base, first) != cudaSuccess) {
+            cudaGetLastError();
+            return bail(FFBF_ENOMEM_DEVICE);
+        }
+        g.bytes = first;
+        g.free_ranges[0] = first;
+        s->segs.push_back(std::move(g));
+        s->arena_held = first;
     }
-    s->arena_bytes = arena_bytes;
-    s->free_ranges[0] = arena_bytes;
     const size_t n_counters = slots + kMaxCtl;
     if (cudaMalloc(&s->d_fast, slots * sizeof(ffbf::FastJob)) != cudaSuccess ||
         cudaMalloc(&s->d_args, slots * sizeof(ffbf::ScanArgs)) != cudaSuccess ||
@@ -532,13 +645,14 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
     // Slots get their scan buffers up front, sized for requests of up to kPreallocText bytes (tile
     // summaries, 64k hit records, pinned copies for 16k hits), so that serving rarely allocates: an
     // allocation inside the loop would synchronise the device and stall every request in flight.
-    const uint64_t prealloc_len = std::min<uint64_t>(arena_bytes, kPreallocText);
+    const uint64_t prealloc_len = kPreallocText;
     for (uint32_t i = 0; i < slots; i++) {
         ffbf_ctx* c = nullptr;
         ffbf_status st = create_scan_slot(device, &c);
         if (st != FFBF_OK) return bail(st);
         s->slots.push_back(c);
-        if ((st = setup_scan_state(c, s->d_arena, prealloc_len)) != FFBF_OK || (st = prepare_fast(c)) != FFBF_OK)
+        // (the pointer only sizes the buffers: nothing is read from it here)
+        if ((st = setup_scan_state(c, s->segs[0].base, prealloc_len)) != FFBF_OK || (st = prepare_fast(c)) != FFBF_OK)
             return bail(st);
         reset_scan(c);
         cudaEvent_t ev;
@@ -558,7 +672,7 @@ ffbf_status ffbf_server_create(int device, uint64_t arena_bytes, uint32_t slots,
         h.cap = kPreallocHits;
         s->free_slots.push_back((int)(slots - 1 - i));
     }
-    s->stats.arena_bytes = arena_bytes;
+    s->stats.arena_bytes = s->arena_held;
     s->stats.slots = slots;
     s->worker = std::thread(worker_loop, s);
     *out = s;
@@ -587,8 +701,9 @@ ffbf_status ffbf_server_submit(ffbf_server* s, uint32_t set_id, const uint8_t* t
     if (!s || !request_id) return FFBF_EINVAL;
     if (set_id >= s->sets.size()) return sfail(s, FFBF_EINVAL, "unknown set");
     if (!text && len) return sfail(s, FFBF_EINVAL, "text is NULL");
-    if ((len + kArenaAlign - 1) / kArenaAlign * kArenaAlign > s->arena_bytes)
-        return sfail(s, FFBF_EINVAL, "request text is larger than the server's text arena");
+    const uint64_t span = (len + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
+    if ((s->arena_cap && span > s->arena_cap) || span + kHbmReserve > s->device_bytes)
+        return sfail(s, FFBF_EINVAL, "request text is larger than the server's text arena can grow");
     Request* r = new (std::nothrow) Request();
     if (!r) return FFBF_ENOMEM_HOST;
     r->set = set_id;

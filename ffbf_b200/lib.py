@@ -370,7 +370,8 @@ class Filter:
         self._check(self._lib.ffbf_debug_scan_unpublished(self._h, ctypes.c_void_p(dev_ptr), n, spins))
 
     def config(self):
-        """(threads, mode) of the tuned scan for this filter (mode 0: shared-memory stage, 1: L2 probes)."""
+        """(threads, mode) of the tuned scan for this filter (mode 0: shared-memory stage, 1: L2 probes, 2:
+        shared-memory stage with candidates deferred to the end of each 32-byte block)."""
         t, m = ctypes.c_int(), ctypes.c_int()
         self._check(self._lib.ffbf_get_scan_config(self._h, ctypes.byref(t), ctypes.byref(m)))
         return t.value, m.value
@@ -472,7 +473,7 @@ class RequestResult:
 
 
 class Server:
-    """Scan server (ffbf_server_*): resident pattern sets, admission by free slots and text-arena room,
+    """Scan server (ffbf_server_*): resident pattern sets, admission by free slots and free device memory,
     continuous batching of the admitted requests on one GPU."""
 
     def __init__(self, device=0, arena_bytes=0, slots=0):

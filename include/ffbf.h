@@ -205,9 +205,14 @@ ffbf_status ffbf_batch_autotune(ffbf_batch* b, size_t sample_bytes, uint32_t* n_
  * sequence (continuous batching). The reference has no counterpart: it scans one corpus per process
  * (ffbf.cpp:529-601); a request here produces what ffbf_scan would for its text and set.
  *
- * ffbf_server_create reserves `arena_bytes` of device memory for request texts (0: half the device's free
- * memory) and `slots` request slots (0: 64), then starts a host thread that runs the loop: admit requests
- * in arrival order while a slot and arena room are free, copy each text to the arena on a copy stream,
+ * ffbf_server_create caps the device memory it holds for request texts at `arena_bytes` (0: no cap) and
+ * takes `slots` request slots (0: 64). The text arena starts as one segment (1 GiB, or the cap if smaller)
+ * and grows in segments while the device's free memory (cudaMemGetInfo, which counts every context's and
+ * process's allocations) stays 1 GiB above what it takes; segments grown beyond the first go back to the
+ * device after a quarter second without admitted requests. A host thread runs the loop: admit requests
+ * in arrival order while a slot and arena room are free (a request that finds neither room nor enough free
+ * device memory waits, and the requests behind it with it, until finished requests or other contexts free
+ * memory), copy each text to the arena on a copy stream,
  * launch every request whose copy has finished as soon as the previous launch sequence is done, and
  * collect each finished request's hits and lines (the line resolution of one batch overlaps the next
  * batch's scan). A request's feed-forward bits go into its set's filter, as successive ffbf_scan calls on
@@ -218,7 +223,8 @@ ffbf_status ffbf_batch_autotune(ffbf_batch* b, size_t sample_bytes, uint32_t* n_
  * text must stay valid until the request is polled; pinned host memory lets its copy overlap other work.
  * ffbf_server_poll returns finished requests (waiting up to wait_us microseconds for the first one);
  * their arrays stay valid until ffbf_server_release. Times are seconds since the server's creation,
- * from the host's steady clock. A request longer than the arena is refused with FFBF_EINVAL. */
+ * from the host's steady clock. A request longer than the cap, or than the device's memory less 1 GiB, is
+ * refused with FFBF_EINVAL. */
 typedef struct ffbf_server ffbf_server;
 typedef struct {
     uint64_t request_id;
@@ -259,8 +265,9 @@ ffbf_status ffbf_autotune(ffbf_ctx* ctx, const uint8_t* d_text, size_t sample_le
  * FFBF_ETIMEOUT and the context stays usable. Nothing is scanned and no result is kept. */
 ffbf_status ffbf_debug_scan_unpublished(ffbf_ctx* ctx, const uint8_t* d_text, size_t len, uint32_t spins);
 
-/* The tuned scan's current configuration for this context (CTA threads; mode 0 shared-memory stage 1,
- * 1 pipelined L2 probes), as the autotuner or the filter's fill chose it. Before the first scan or tuning
+/* The tuned scan's current configuration for this context (CTA threads; mode 0 shared-memory stage 1 with
+ * candidates queued per byte, 1 pipelined L2 probes, 2 shared-memory stage 1 with candidates deferred to the
+ * end of each 32-byte block), as the autotuner or the filter's fill chose it. Before the first scan or tuning
  * it reports the defaults. */
 ffbf_status ffbf_get_scan_config(const ffbf_ctx* ctx, int* threads, int* mode);
 

@@ -145,3 +145,54 @@ def test_server_refuses_request_larger_than_arena():
             with Filter(prm) as g:
                 with pytest.raises(FFBFError):
                     srv.add_set(g)
+
+
+def test_server_admission_waits_for_device_memory():
+    """Admission follows the device's free memory, which every context's allocations reduce: while another
+    allocation holds nearly all of it, a request larger than the room the server already holds waits (it is
+    not refused and does not fail) and a request that fits that room still runs; once the memory is freed the
+    waiting request is admitted and its results equal a plain ffbf_scan of its text. Room grown for it goes
+    back to the device after the server has been idle for a while."""
+    import torch
+
+    prm, pats, text = build_inputs("plain_small")
+    reps = (1280 << 20) // text.size + 1
+    big = np.ascontiguousarray(np.tile(text, reps))  # ~1.25 GiB: more than the server's first segment
+    small = text[: 1 << 20]
+    with Filter(prm) as g:
+        g.add_patterns(pats)
+        want_big = g.process(big)
+        want_small = g.process(small)
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        with Server(0, arena_bytes=0, slots=4) as srv:
+            sid = srv.add_set(f)
+            first = srv.stats()["arena_bytes"]
+            assert first < big.size
+            free, _ = torch.cuda.mem_get_info()
+            blocker = torch.empty(free - (1536 << 20), dtype=torch.uint8, device="cuda")
+            try:
+                rid_small = srv.submit(sid, small)
+                got = drain(srv, 1)
+                assert got[rid_small].status == 0
+                np.testing.assert_array_equal(got[rid_small].hit_offsets, want_small.hit_offsets)
+                rid_big = srv.submit(sid, big)
+                t_end = time.time() + 1.0
+                while time.time() < t_end:
+                    assert not srv.poll(wait_us=50_000), "the large request ran while the memory was held"
+                assert srv.stats()["arena_bytes"] == first
+            finally:
+                del blocker
+                torch.cuda.empty_cache()
+            got = drain(srv, 1)
+            r = got[rid_big]
+            assert r.status == 0
+            np.testing.assert_array_equal(r.hit_offsets, want_big.hit_offsets)
+            np.testing.assert_array_equal(r.line_start, want_big.line_start)
+            np.testing.assert_array_equal(r.line_end, want_big.line_end)
+            assert r.t_admit - r.t_submit >= 0.9, "admission should have waited for the memory"
+            assert srv.stats()["arena_bytes"] > first
+            t_end = time.time() + 5.0
+            while srv.stats()["arena_bytes"] > first and time.time() < t_end:
+                time.sleep(0.05)
+            assert srv.stats()["arena_bytes"] == first, "grown room should go back to the device when idle"
