@@ -6,7 +6,7 @@
 // per stream (from a 32-byte halo) instead of once per tile.
 //
 // Staging. Row r of the CTA's streams is loaded by TMA as 3-D boxes {128 bytes, 1 row, <=256 streams}
-// (cp.async.bulk.tensor, 128B swizzle, no multicast) into a double-buffered shared-memory stage completed on
+// (cp.async.bulk.tensor, 128B swizzle, one CTA per load) into a double-buffered shared-memory stage completed on
 // an mbarrier. The 128B swizzle puts chunk c of thread t's row at chunk c ^ (t & 7), so the 16-byte reads
 // of a quarter-warp hit eight different bank groups.
 //
