@@ -146,3 +146,33 @@ def test_bench_pattern_override_names_its_own_workload(monkeypatch):
     assert wl.name == "scale_200k" and wl.n_patterns == 200000 and wl.text_bytes == 1 << 20
     assert b.profiled_traffic_ratio(wl.name) is None
     assert b.describe(wl)["workload"].startswith("scale_200k: 200000 patterns")
+
+
+def test_reference_arm_runs_the_whole_text_without_repository_libraries(tmp_path):
+    """bench.py --impl reference needs no GPU: the reference binary scans the whole workload text in
+    line-aligned shards, and the arm's own process maps none of this repository's shared libraries (a child
+    process writes the inputs)."""
+    import json
+    import sys
+
+    from ffbf_b200 import datagen
+    if oracle.ref_binary(datagen.plain().params) is None:
+        pytest.skip("reference binary for the plain geometry not built (oracle/_ref)")
+    probe = tmp_path / "arm.py"
+    probe.write_text(
+        "import json, sys\n"
+        f"sys.path.insert(0, {ROOT!r})\n"
+        "sys.argv = ['bench.py', '--impl', 'reference', '--workload', 'plain', '--steps', '1', '--warmup', '0']\n"
+        "import bench\n"
+        "bench.main_reference(bench.parse())\n"
+        "maps = open('/proc/self/maps').read().split('\\n')\n"
+        f"mine = sorted({{m.split()[-1] for m in maps if {ROOT!r} in m and m.endswith('.so')}})\n"
+        "print(json.dumps({'repo_libraries': mine}))\n")
+    out = subprocess.run([sys.executable, str(probe)], capture_output=True, text=True, cwd=ROOT, timeout=600)
+    assert out.returncode == 0, out.stderr[-2000:]
+    lines = [json.loads(x) for x in out.stdout.strip().splitlines()]
+    arm, maps = lines[-2], lines[-1]
+    assert arm["impl"] == "reference" and arm["value"] > 0
+    assert arm["config"]["text_bytes"] == 64 << 20
+    assert "whole" in arm["cpu_baseline"]["sample"]
+    assert maps["repo_libraries"] == []
