@@ -87,7 +87,7 @@ struct ffbf_server {
         uint64_t bytes = 0;
         std::map<uint64_t, uint64_t> free_ranges;  // offset -> length, coalesced
     };
-    std::vector<Segment> segs;    // segs[0] lives as long as the server
+    std::vector<Segment> segs;    // segs[0] is kept while the server idles (at its first size)
     uint64_t arena_cap = 0;       // most arena bytes the server holds (0: bounded by free device memory only)
     uint64_t arena_held = 0;      // bytes of all segments
     uint64_t device_bytes = 0;    // the device's memory
@@ -231,8 +231,13 @@ bool arena_alloc(ffbf_server* s, uint64_t bytes, int* seg, uint64_t* off) {
 
 void arena_free(ffbf_server* s, int seg, uint64_t off, uint64_t bytes) { seg_free(s->segs[seg], off, bytes); }
 
-// With nothing admitted, the segments grown for earlier requests go back to the device (cudaFree waits for
-// the device, which is idle then).
+uint64_t first_segment_bytes(const ffbf_server* s) {
+    return s->arena_cap ? std::min(s->arena_cap, kSegmentBytes) : kSegmentBytes;
+}
+
+// With nothing admitted, the segments grown for earlier requests go back to the device, and a first segment
+// that was rebuilt larger for one request returns to its first size (cudaFree waits for the device, which is
+// idle then).
 void arena_shrink(ffbf_server* s) {
     bool freed = false;
     while (s->segs.size() > 1) {
@@ -243,11 +248,68 @@ void arena_shrink(ffbf_server* s) {
         s->segs.pop_back();
         freed = true;
     }
+    if (s->segs.size() == 1 && s->segs[0].bytes > first_segment_bytes(s) && s->segs[0].free_ranges.size() == 1 &&
+        s->segs[0].free_ranges.begin()->second == s->segs[0].bytes) {
+        auto& g = s->segs[0];
+        cudaFree(g.base);
+        s->arena_held -= g.bytes;
+        g.bytes = first_segment_bytes(s);
+        g.free_ranges.clear();
+        if (cudaMalloc(&g.base, g.bytes) != cudaSuccess) {
+            cudaGetLastError();
+            s->segs.clear();  // the next admission grows a segment as memory allows
+        } else {
+            g.free_ranges[0] = g.bytes;
+            s->arena_held += g.bytes;
+        }
+        freed = true;
+    }
     if (freed) {
         cudaGetLastError();
         std::lock_guard<std::mutex> lk(s->mu);
         s->stats.arena_bytes = s->arena_held;
     }
+}
+
+// With nothing admitted (so every segment is free), the arena is replaced by one segment that holds `bytes`:
+// free segments that are each too small, or a cap that the existing segments already fill, would otherwise
+// keep a request that fits the cap waiting for good. The server's own segments count as free memory here.
+bool arena_rebuild(ffbf_server* s, uint64_t bytes) {
+    const double t = s->now();
+    if (s->last_grow_fail >= 0 && t - s->last_grow_fail < kGrowRetrySeconds) return false;
+    uint64_t want = std::max(bytes, first_segment_bytes(s));
+    if (s->arena_cap) want = std::min(want, s->arena_cap);
+    size_t free_b = 0, total_b = 0;
+    if (cudaMemGetInfo(&free_b, &total_b) != cudaSuccess || free_b + s->arena_held < want + kHbmReserve) {
+        cudaGetLastError();
+        s->last_grow_fail = t;
+        return false;
+    }
+    for (auto& g : s->segs) cudaFree(g.base);
+    s->segs.clear();
+    s->arena_held = 0;
+    ffbf_server::Segment g;
+    if (cudaMalloc(&g.base, want) != cudaSuccess) {
+        cudaGetLastError();
+        s->last_grow_fail = t;
+        std::lock_guard<std::mutex> lk(s->mu);
+        s->stats.arena_bytes = 0;
+        return false;  // the next admission grows a segment as memory allows
+    }
+    g.bytes = want;
+    g.free_ranges[0] = want;
+    s->segs.push_back(std::move(g));
+    s->arena_held = want;
+    s->last_grow_fail = -1.0;
+    std::lock_guard<std::mutex> lk(s->mu);
+    s->stats.arena_bytes = s->arena_held;
+    return true;
+}
+
+// No request holds a slot: nothing is copying, ready, on the device or being collected.
+bool nothing_admitted(const ffbf_server* s) {
+    return s->copying.empty() && s->ready.empty() && !s->in_flight && s->resolving.empty() && s->slow.empty() &&
+           s->running.empty();
 }
 
 // Ends a request: its slot and arena range return to the pools and it joins the finished queue.
@@ -271,7 +333,9 @@ void admit(ffbf_server* s) {
         const uint64_t span = (r->len + kArenaAlign - 1) / kArenaAlign * kArenaAlign;
         uint64_t off = 0;
         int seg = 0;
-        if (span && !arena_alloc(s, span, &seg, &off)) break;  // in order: wait for room
+        if (span && !arena_alloc(s, span, &seg, &off) &&
+            !(nothing_admitted(s) && arena_rebuild(s, span) && arena_alloc(s, span, &seg, &off)))
+            break;  // in order: wait for room
         s->pending.pop_front();
         r->slot = s->free_slots.back();
         s->free_slots.pop_back();
@@ -522,11 +586,12 @@ void worker_loop(ffbf_server* s) {
             progress = true;
         }
         // With nothing admitted for a while, segments grown for earlier requests go back to the device.
-        const bool quiet = s->copying.empty() && s->ready.empty() && !s->in_flight && s->resolving.empty() &&
-                           s->slow.empty() && s->running.empty();
+        const bool quiet = nothing_admitted(s);
         if (quiet && s->pending.empty()) {
             if (s->idle_since < 0) s->idle_since = s->now();
-            else if (s->segs.size() > 1 && s->now() - s->idle_since > kShrinkIdleSeconds) arena_shrink(s);
+            else if ((s->segs.size() > 1 || (s->segs.size() == 1 && s->segs[0].bytes > first_segment_bytes(s))) &&
+                     s->now() - s->idle_since > kShrinkIdleSeconds)
+                arena_shrink(s);
         } else {
             s->idle_since = -1.0;
         }

@@ -149,7 +149,7 @@ def test_server_refuses_request_larger_than_arena():
 
 def test_server_admission_waits_for_device_memory():
     """Admission follows the device's free memory, which every context's allocations reduce: while another
-    allocation holds nearly all of it, a request larger than the room the server already holds waits (it is
+    allocation holds all but 1 GiB of it, a request larger than the room the server already holds waits (it is
     not refused and does not fail) and a request that fits that room still runs; once the memory is freed the
     waiting request is admitted and its results equal a plain ffbf_scan of its text. Room grown for it goes
     back to the device after the server has been idle for a while."""
@@ -170,7 +170,9 @@ def test_server_admission_waits_for_device_memory():
             first = srv.stats()["arena_bytes"]
             assert first < big.size
             free, _ = torch.cuda.mem_get_info()
-            blocker = torch.empty(free - (1536 << 20), dtype=torch.uint8, device="cuda")
+            # 1 GiB stays free: the server may neither add a segment for the large text nor replace its first
+            # one, since either would leave less than its 1 GiB reserve
+            blocker = torch.empty(free - (1 << 30), dtype=torch.uint8, device="cuda")
             try:
                 rid_small = srv.submit(sid, small)
                 got = drain(srv, 1)
@@ -196,3 +198,29 @@ def test_server_admission_waits_for_device_memory():
             while srv.stats()["arena_bytes"] > first and time.time() < t_end:
                 time.sleep(0.05)
             assert srv.stats()["arena_bytes"] == first, "grown room should go back to the device when idle"
+
+
+def test_server_cap_admits_a_request_larger_than_its_first_segment():
+    """With a cap of 2 GiB the arena starts as one 1 GiB segment and may not grow past the cap by adding a
+    second one, so a 1.5 GiB request is admitted by replacing the idle arena with one segment that holds it;
+    once the server idles again the arena returns to its first size."""
+    prm, pats, text = build_inputs("plain_small")
+    big = np.ascontiguousarray(np.tile(text, (1536 << 20) // text.size + 1)[: 1536 << 20])
+    with Filter(prm) as g:
+        g.add_patterns(pats)
+        want = g.process(big)
+    with Filter(prm) as f:
+        f.add_patterns(pats)
+        with Server(0, arena_bytes=2 << 30, slots=2) as srv:
+            sid = srv.add_set(f)
+            first = srv.stats()["arena_bytes"]
+            assert first == 1 << 30
+            rid = srv.submit(sid, big)
+            r = drain(srv, 1)[rid]
+            assert r.status == 0
+            np.testing.assert_array_equal(r.hit_offsets, want.hit_offsets)
+            np.testing.assert_array_equal(r.line_start, want.line_start)
+            t_end = time.time() + 5.0
+            while srv.stats()["arena_bytes"] != first and time.time() < t_end:
+                time.sleep(0.05)
+            assert srv.stats()["arena_bytes"] == first
