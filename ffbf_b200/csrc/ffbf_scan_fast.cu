@@ -627,6 +627,11 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                         if (row_first < 0 && need_first) row_first = 32 * b + __ffs(nlm) - 1;
                     }
                 } else {
+                    // MODE 0 tests each window one byte late: the table words of byte j are loaded, then byte
+                    // j - 1's (loaded a byte earlier) are tested and queued, so the shared-memory latency of a
+                    // byte's probes overlaps the next byte's hash instead of stalling before its warp vote
+                    uint32_t pw0 = 0, pw1 = 0, pl = 0, ph = 0;
+                    bool pv = false;
 #pragma unroll
                     for (int j = 0; j < 32; j++) {
                         const uint32_t c = byte_at(cur[j >> 2], j & 3);
@@ -644,10 +649,18 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                         if constexpr (MODE == 0) {
                             const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
                             const uint32_t w1 = lds32(s1 + ((hh >> 3) & s1_bmask));
-                            // both table bits in one test (the second is forced on when S = 1)
-                            const uint32_t t = __funnelshift_r(w0, w0, hl) & (__funnelshift_r(w1, w1, hh) | one_probe);
-                            const bool pass = (j - lnp >= L) && (t & 1u) != 0;
-                            enqueue(pass, (uint32_t)(kRowBytes + 32 * b + j), hl, hh, s1_first);
+                            const bool valid = j - lnp >= L;
+                            if (j > 0) {
+                                // both table bits in one test (the second is forced on when S = 1)
+                                const uint32_t t =
+                                    __funnelshift_r(pw0, pw0, pl) & (__funnelshift_r(pw1, pw1, ph) | one_probe);
+                                enqueue(pv && (t & 1u) != 0, (uint32_t)(kRowBytes + 32 * b + j - 1), pl, ph, s1_first);
+                            }
+                            pw0 = w0;
+                            pw1 = w1;
+                            pl = hl;
+                            ph = hh;
+                            pv = valid;
                         } else {
                             const int slot = j % kRing;
                             // stage B: the window that entered stage A 2*kRing bytes ago (a probe's bit sits at
@@ -677,6 +690,10 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                             else
                                 ring_v[slot] = ldg_if(main_words + (((fa & a_mask) + a_add) >> 5), issue);
                         }
+                    }
+                    if constexpr (MODE == 0) {  // the block's last window
+                        const uint32_t t = __funnelshift_r(pw0, pw0, pl) & (__funnelshift_r(pw1, pw1, ph) | one_probe);
+                        enqueue(pv && (t & 1u) != 0, (uint32_t)(kRowBytes + 32 * b + 31), pl, ph, s1_first);
                     }
                 }
                 if (MODE != 4 && lnp != lnp_blk && row_first < 0 && need_first) {
