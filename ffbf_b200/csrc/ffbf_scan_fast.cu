@@ -632,14 +632,33 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
                     // byte's probes overlaps the next byte's hash instead of stalling before its warp vote
                     uint32_t pw0 = 0, pw1 = 0, pl = 0, ph = 0;
                     bool pv = false;
+                    // S-box entries of byte j's incoming and outgoing bytes; MODE 0 loads them a byte ahead
+                    auto sbox_in = [&](int j) { return lds64(lane_tab + byte_at(cur[j >> 2], j & 3) * 128u); };
+                    auto sbox_out = [&](int j) {
+                        const uint32_t co = j >= L ? byte_at(cur[(j - L) >> 2], (j - L) & 3)
+                                                   : byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
+                        return lds64(lane_tab + co * 128u);
+                    };
+                    uint2 nsv = make_uint2(0, 0), no = make_uint2(0, 0);
+                    if constexpr (MODE == 0) {
+                        nsv = sbox_in(0);
+                        no = sbox_out(0);
+                    }
 #pragma unroll
                     for (int j = 0; j < 32; j++) {
                         const uint32_t c = byte_at(cur[j >> 2], j & 3);
-                        uint32_t co;
-                        if (j >= L) co = byte_at(cur[(j - L) >> 2], (j - L) & 3);
-                        else co = byte_at(prev[(j - L + 32) >> 2], (j - L + 32) & 3);
-                        const uint2 sv = lds64(lane_tab + c * 128u);
-                        const uint2 o = lds64(lane_tab + co * 128u);
+                        uint2 sv, o;
+                        if constexpr (MODE == 0) {
+                            sv = nsv;
+                            o = no;
+                            if (j + 1 < 32) {
+                                nsv = sbox_in(j + 1);
+                                no = sbox_out(j + 1);
+                            }
+                        } else {
+                            sv = sbox_in(j);
+                            o = sbox_out(j);
+                        }
                         uint32_t rl, rh;
                         rol_pair<L>(o.x, o.y, rl, rh);
                         const uint32_t nl = __funnelshift_l(hh, hl, 1), nh = __funnelshift_l(hl, hh, 1);
