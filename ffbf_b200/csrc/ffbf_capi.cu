@@ -208,8 +208,9 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         if (!c->cfg_tuned) {
             c->cfg.mode = c->force_mode >= 0 ? c->force_mode : c->stage1_fill > 0.3 ? 1 : 0;
             // default CTA sizes (measured best on the 10k- and 1M-pattern workloads): 512 threads for the
-            // shared-memory stage, 384 for dense filters
-            c->cfg.threads = c->threads_env ? c->threads_env : c->cfg.mode == 1 ? 384 : c->cfg.mode == 2 ? 256 : 512;
+            // shared-memory stage, 2 x 192 per SM for dense filters
+            // (dense: two 192-thread CTAs per SM; probe order 2 needs the 384-thread CTA's room for its table)
+            c->cfg.threads = c->threads_env ? c->threads_env : c->cfg.mode == 1 ? 192 : c->cfg.mode == 2 ? 256 : 512;
         }
         c->stage1_dirty = false;
     }

@@ -283,8 +283,12 @@ __device__ __forceinline__ uint32_t newline_mask32(const uint32_t (&w)[8]) {
     return m;
 }
 
+// CTAs per SM: the dense modes at 192 threads run two CTAs per SM (12 warps, as one 384-thread CTA, but two
+// independent pipelines and barriers of 6 warps each); every other configuration runs one.
+__host__ __device__ constexpr int ctas_per_sm(int threads, int mode) { return threads == 192 && mode >= 1 && mode <= 3 ? 2 : 1; }
+
 template <int L, int THREADS, int MODE>
-__global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
+__global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
                                                           uint32_t n_items, uint32_t max_s1_words,
                                                           uint32_t* __restrict__ ctl) {
     // ctl[0]: error flags; ctl[1]: the work queue, the count of items handed out past the first wave
@@ -294,7 +298,7 @@ __global__ void __launch_bounds__(THREADS, 1) k_scan_fast(const FastJob* __restr
     constexpr int kQBytes = kQCap * 16;
     // dense mode: ring depth per stage (divides 32); 384-thread CTAs trade depth for warps (more L2 probes
     // in flight per SM within the register file)
-    constexpr int kRing = THREADS >= 384 ? 4 : 8;
+    constexpr int kRing = THREADS >= 384 || ctas_per_sm(THREADS, MODE) == 2 ? 4 : 8;
     constexpr int kBox = THREADS > 256 ? THREADS / 2 : THREADS;  // streams per TMA box (<= 256)
     constexpr bool kTable = MODE == 0 || MODE == 3 || MODE == 4;  // reads the stage-1 table
     extern __shared__ uint8_t smem_raw[];
@@ -809,7 +813,8 @@ cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
     cudaError_t e =
         cudaFuncSetAttribute(k_scan_fast<L, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
-    const int grid = (int)(n_items < (uint32_t)num_sms ? n_items : (uint32_t)num_sms);
+    const uint32_t slots = (uint32_t)num_sms * (uint32_t)ctas_per_sm(THREADS, MODE);
+    const int grid = (int)(n_items < slots ? n_items : slots);
     if (grid == 0) return cudaSuccess;
     k_scan_fast<L, THREADS, MODE><<<grid, THREADS, smem, st>>>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl);
     note_launches(1);
@@ -819,7 +824,10 @@ cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
 template <int L>
 cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items,
                        uint32_t max_s1_words, uint32_t* d_ctl, int num_sms, cudaStream_t st) {
-    if (cfg.mode == 1) {  // dense: 384 threads (ring depth 4) or 256 (depth 8); 512 would spill
+    if (cfg.mode == 1) {  // dense: 384 threads (ring depth 4), 256 (depth 8) or 2 x 192 (depth 4); 512 would spill
+        if (cfg.threads == 192 && cfg.order != 2)
+            return cfg.order == 1 ? launch_cfg<L, 192, 2>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
+                                  : launch_cfg<L, 192, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
         if (cfg.order == 1)
             return cfg.threads == 256 ? launch_cfg<L, 256, 2>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
                                       : launch_cfg<L, 384, 2>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
@@ -845,7 +853,7 @@ cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_
 }
 
 size_t fixed_smem_for(int threads, bool dense) {
-    if (dense) return threads == 256 ? fixed_smem<256, 1>() : fixed_smem<384, 1>();
+    if (dense) return threads == 256 ? fixed_smem<256, 1>() : threads == 192 ? fixed_smem<192, 1>() : fixed_smem<384, 1>();
     switch (threads) {
         case 192: return fixed_smem<192, 0>();
         case 256: return fixed_smem<256, 0>();
@@ -906,7 +914,7 @@ int dense_probe_order(const Geom& g, double cache_fill, double ext_fill) {
 }
 
 int config_threads(const FastConfig& cfg) {
-    if (cfg.mode == 1) return cfg.threads == 256 ? 256 : 384;
+    if (cfg.mode == 1) return cfg.threads == 256 ? 256 : cfg.threads == 192 && cfg.order != 2 ? 192 : 384;
     if (cfg.mode == 2) return cfg.threads == 192 || cfg.threads == 384 ? cfg.threads : 256;
     return cfg.threads == 384 || cfg.threads == 512 ? cfg.threads : 256;
 }

@@ -184,6 +184,9 @@ SCAN_VARIANTS = [
     {"FFBF_SCAN_MODE": "2", "FFBF_SCAN_THREADS": "384"},
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0", "FFBF_SCAN_THREADS": "256"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0", "FFBF_SCAN_THREADS": "192"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "192"},
+    {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "2", "FFBF_SCAN_THREADS": "192"},
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"},
     {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "2"},
@@ -231,6 +234,7 @@ def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
     variants = [{}, {"FFBF_SCAN_MODE": "2"}, {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"},
+                {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "192"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "2"}]
     for env in variants:
         for key in SCAN_ENV:
