@@ -79,7 +79,7 @@ ffbf_status build_plan(const std::vector<PlanJob>& jobs, int num_sms, ScanPlan& 
             const ffbf::FastConfig cfg = c->cfg;
             const int threads = ffbf::config_threads(cfg);
             // in a batch other jobs fill the GPU, so rows per stream follow this job's size alone
-            const uint32_t rows = cfg.rows ? cfg.rows : ffbf::fast_rows(a.n, threads, num_sms, true);
+            const uint32_t rows = cfg.rows ? cfg.rows : ffbf::fast_rows(a.n, cfg, num_sms, true);
             ffbf::FastJob fj;
             cudaError_t e;
             covered = ffbf::fill_fast_job(a, c->d_stage1, cfg, rows, &fj, &e);
@@ -449,7 +449,7 @@ ffbf_status autotune_impl(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
         if (per_sm) {
             const int t = ffbf::config_threads(cand);
             const uint64_t bytes = sample_len / ffbf::kScanTile * ffbf::kScanTile;
-            const uint64_t streams = bytes / ((uint64_t)ffbf::fast_rows(sample_len, t, c->num_sms, false) * 128);
+            const uint64_t streams = bytes / ((uint64_t)ffbf::fast_rows(sample_len, cand, c->num_sms, false) * 128);
             const uint64_t items = (streams + t - 1) / t;
             score = ms * (double)std::min<uint64_t>(items, (uint64_t)c->num_sms);
         }

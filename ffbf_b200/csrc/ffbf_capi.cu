@@ -737,7 +737,7 @@ ffbf_status scan_host_pipelined(ffbf_ctx* c, const uint8_t* text, size_t len) {
     c->scan_path = 1;
     const ffbf::ScanArgs a = make_scan_args(c);
     const int threads = ffbf::config_threads(c->cfg);
-    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(len, threads, c->num_sms, false);
+    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(len, c->cfg, c->num_sms, false);
     ffbf::FastJob job;
     cudaError_t e;
     const uint64_t covered = ffbf::fill_fast_job(a, c->d_stage1, c->cfg, rows, &job, &e);
@@ -1179,7 +1179,7 @@ ffbf_status ffbf_debug_scan_unpublished(ffbf_ctx* c, const uint8_t* d_text, size
     TRY(prepare_fast(c));
     const ffbf::ScanArgs a = make_scan_args(c);
     const int threads = ffbf::config_threads(c->cfg);
-    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(len, threads, c->num_sms, false);
+    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(len, c->cfg, c->num_sms, false);
     cudaError_t e;
     ffbf::fill_fast_job(a, c->d_stage1, c->cfg, rows, c->h_job, &e);
     if (e != cudaSuccess) return fail(c, FFBF_ECUDA, "tensor map encoding failed");

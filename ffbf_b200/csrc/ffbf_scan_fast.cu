@@ -919,17 +919,32 @@ int config_threads(const FastConfig& cfg) {
     return cfg.threads == 384 || cfg.threads == 512 ? cfg.threads : 256;
 }
 
-uint32_t fast_rows(uint64_t n, int threads, int num_sms, bool batch) {
+int fast_ctas_per_sm(const FastConfig& cfg) { return cfg.mode == 1 && config_threads(cfg) == 192 ? 2 : 1; }
+
+uint32_t fast_rows(uint64_t n, const FastConfig& cfg, int num_sms, bool batch) {
+    const int threads = config_threads(cfg);
     const uint64_t tiles_bytes = n / kScanTile * kScanTile;
-    uint32_t rows = 16;
     if (batch) {
         // in a batch other jobs fill the GPU: the largest tile this job still fills four times over
+        uint32_t rows = 16;
         while (rows > 4 && tiles_bytes < 4ull * rows * kRowBytes * threads) rows >>= 1;
-    } else {
-        // alone: enough supertiles for several per SM
-        while (rows > 4 && tiles_bytes / ((uint64_t)rows * kRowBytes * threads) < 4ull * num_sms) rows >>= 1;
+        return rows;
     }
-    return rows;
+    // alone: the CTAs take items round robin, so the scan lasts as many waves of items as the busiest CTA
+    // takes, and each item loads its rows plus one halo row. The row count with the fewest row loads per
+    // CTA wins; ties go to the longer items.
+    const uint64_t slots = (uint64_t)num_sms * (uint64_t)fast_ctas_per_sm(cfg);
+    uint32_t best = 16;
+    uint64_t best_loads = ~0ull;
+    for (uint32_t rows = 16; rows >= 4; rows >>= 1) {
+        const uint64_t items = (tiles_bytes / ((uint64_t)rows * kRowBytes) + threads - 1) / threads;
+        const uint64_t loads = (items + slots - 1) / slots * (rows + 1);
+        if (loads < best_loads) {
+            best_loads = loads;
+            best = rows;
+        }
+    }
+    return best;
 }
 
 uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const FastConfig& cfg, uint32_t rows,
@@ -1020,7 +1035,7 @@ cudaError_t scan_tail(const ScanArgs& a, uint64_t covered, cudaStream_t st) {
 cudaError_t scan_fast(const ScanArgs& a, const uint32_t* stage1_words, const FastConfig& cfg, int num_sms,
                       FastJob* h_job, FastJob* d_job, cudaStream_t st) {
     const int threads = config_threads(cfg);
-    const uint32_t rows = cfg.rows ? cfg.rows : fast_rows(a.n, threads, num_sms, false);
+    const uint32_t rows = cfg.rows ? cfg.rows : fast_rows(a.n, cfg, num_sms, false);
     cudaError_t e;
     const uint64_t covered = fill_fast_job(a, stage1_words, cfg, rows, h_job, &e);
     if (e != cudaSuccess) return e;

@@ -70,8 +70,11 @@ uint32_t stage1_words_for(const Geom& g, int threads, bool dense = false);
 cudaError_t build_stage1(const uint32_t* main_words, const Geom& g, int threads, bool dense, uint32_t* out,
                          cudaStream_t st);
 
+// CTAs of the tuned kernel resident per SM for a configuration (two for the 192-thread dense kernel).
+int fast_ctas_per_sm(const FastConfig& cfg);
+
 // Rows per stream for a text of n bytes, alone on the GPU or in a batch.
-uint32_t fast_rows(uint64_t n, int threads, int num_sms, bool batch);
+uint32_t fast_rows(uint64_t n, const FastConfig& cfg, int num_sms, bool batch);
 
 // Fills *job (host memory) for the whole 16 KiB tiles of a.text and returns the bytes it covers; the
 // caller sets item_begin. scan_tail runs the generic kernel over the tiles from `covered` on.
