@@ -375,7 +375,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
         s_nr = -1;
         mbar_init(bar0, 1);
         mbar_init(bar1, 1);
-        *reinterpret_cast<uint32_t*>(smem + (bar0 - base) + 64) = 0xFFFFFFFFu;  // MODE 4's one-probe word
+        *reinterpret_cast<uint32_t*>(smem + (bar0 - base) + 64) = 0xFFFFFFFFu;  // the S = 1 second-probe word
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         // publication gate: a bounded poll, and no load in flight if it gives up
         bool open = true;
@@ -402,7 +402,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
 
     // the current job's parameters (reloaded when the job changes)
     int cur_job = -1;
-    uint32_t R = 0, s1_bmask = 0, s1_first = 0, spt_log2 = 0, one_probe = 0;
+    uint32_t R = 0, s1_bmask = 0, s1_first = 0, spt_log2 = 0;
     uint32_t a_mask = 0, a_add = 0, b_mask = 0, b_add = 0;  // dense mode: regions of the two pipelined probes
     bool two = false;
     auto job_desc = [&]() { return jobs + cur_job; };
@@ -447,7 +447,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
     int lnp = -1000;  // last '\n' relative to the current row start
     uint32_t prev[8] = {0, 0, 0, 0, 0, 0, 0, 0};
     // MODE 4: newline mask of the previous block (bit 31 forced at the text's start, where nothing precedes
-    // offset 0), and the second probe's table (the stage-1 table, or with S = 1 a word of ones: one probe)
+    // offset 0). MODE 0 and 4: the second probe's table (the stage-1 table, or with S = 1 a word of ones)
     uint32_t nl_prev = 0;
     uint32_t s2 = s1, s2_bmask = 0;
 
@@ -487,7 +487,6 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
             s1_fits = !kTable || J->stage1_nwords <= max_s1_words;
             const uint32_t cmask = g.cache_mask;
             two = g.s > 1;
-            one_probe = two ? 0u : 1u;
             // stage-1 table of T = C >> shift bits, folded modulo T: the byte offset of bit (h & (T-1))'s
             // word is (h >> 3) & s1_bmask
             s1_bmask = (((cmask >> J->stage1_shift) >> 3) & ~3u);
@@ -670,13 +669,12 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                         hh = nh ^ sv.y ^ rh;
                         if (c == 0x0Au) lnp = j;
                         if constexpr (MODE == 0) {
+                            // with S = 1 the second probe reads a word of ones
                             const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
-                            const uint32_t w1 = lds32(s1 + ((hh >> 3) & s1_bmask));
+                            const uint32_t w1 = lds32(s2 + ((hh >> 3) & s2_bmask));
                             const bool valid = j - lnp >= L;
                             if (j > 0) {
-                                // both table bits in one test (the second is forced on when S = 1)
-                                const uint32_t t =
-                                    __funnelshift_r(pw0, pw0, pl) & (__funnelshift_r(pw1, pw1, ph) | one_probe);
+                                const uint32_t t = __funnelshift_r(pw0, pw0, pl) & __funnelshift_r(pw1, pw1, ph);
                                 enqueue(pv && (t & 1u) != 0, (uint32_t)(kRowBytes + 32 * b + j - 1), pl, ph, s1_first);
                             }
                             pw0 = w0;
@@ -715,7 +713,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                         }
                     }
                     if constexpr (MODE == 0) {  // the block's last window
-                        const uint32_t t = __funnelshift_r(pw0, pw0, pl) & (__funnelshift_r(pw1, pw1, ph) | one_probe);
+                        const uint32_t t = __funnelshift_r(pw0, pw0, pl) & __funnelshift_r(pw1, pw1, ph);
                         enqueue(pv && (t & 1u) != 0, (uint32_t)(kRowBytes + 32 * b + 31), pl, ph, s1_first);
                     }
                 }
@@ -930,17 +928,18 @@ uint32_t fast_rows(uint64_t n, const FastConfig& cfg, int num_sms, bool batch) {
         while (rows > 4 && tiles_bytes < 4ull * rows * kRowBytes * threads) rows >>= 1;
         return rows;
     }
-    // alone: the CTAs take items round robin, so the scan lasts as many waves of items as the busiest CTA
-    // takes, and each item loads its rows plus one halo row. The row count with the fewest row loads per
-    // CTA wins; ties go to the longer items.
+    // alone: the scan lasts as many waves of equal items as the busiest CTA takes, and an item costs its
+    // rows plus its halo, whose 32 hashed bytes are a quarter of a row's work (measured: 256 MiB of the
+    // plain workload, 2 waves of 16 rows against 7 of 4, took 571 against 528 us). The row count with the
+    // least work per CTA wins; ties go to the longer items.
     const uint64_t slots = (uint64_t)num_sms * (uint64_t)fast_ctas_per_sm(cfg);
     uint32_t best = 16;
-    uint64_t best_loads = ~0ull;
+    uint64_t best_cost = ~0ull;
     for (uint32_t rows = 16; rows >= 4; rows >>= 1) {
         const uint64_t items = (tiles_bytes / ((uint64_t)rows * kRowBytes) + threads - 1) / threads;
-        const uint64_t loads = (items + slots - 1) / slots * (rows + 1);
-        if (loads < best_loads) {
-            best_loads = loads;
+        const uint64_t cost = (items + slots - 1) / slots * (4 * rows + 1);  // in quarter rows
+        if (cost < best_cost) {
+            best_cost = cost;
             best = rows;
         }
     }

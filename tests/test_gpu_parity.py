@@ -223,7 +223,8 @@ def test_scan_variants_agree_with_oracle(name, monkeypatch):
                                    (32, 5, 1), (16, 6, 2), (19, 11, 0)])
 def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
     """The dense mode pipelines two probes: f0/f1 (order 0), f2/f3 (order 1, K >= 4), or f0/f1 behind a
-    shared-memory prefilter of f0 (order 2). Each geometry's regions decide where those probes land (cache or
+    shared-memory prefilter of f0 (order 2). The shared-memory mode runs here too, at both CTA sizes, with
+    S = 1 (one stage-1 probe) and S >= 2 (two). Each geometry's regions decide where those probes land (cache or
     external) and which queued windows still need which probes; K = 1 has no second index function and falls
     back to the shared-memory mode."""
     from cases import _gen
@@ -231,7 +232,8 @@ def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
     prm = Params(L, k, s, 1 << 14, 1 << 16)  # small regions: dense fills, many false positives
     pats, text = _gen(40 + k * 3 + s, dg.PRINTABLE, 3000, L, L + 16, 2_000_000, 80, 300)
     o, so, _, _, _ = run_oracle(prm, pats, text)
-    variants = [{}, {"FFBF_SCAN_MODE": "2"}, {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
+    variants = [{}, {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "384"}, {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "512"},
+                {"FFBF_SCAN_MODE": "2"}, {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "192"},
