@@ -23,7 +23,7 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 NVFLAGS = ARCH + ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xcompiler", "-Wall",
                   f"-I{os.path.join(ROOT, 'include')}"]
 
-CUDA_SOURCES = ["ffbf_kernels.cu", "ffbf_scan_fast.cu", "ffbf_capi.cu", "ffbf_batch.cu", "ffbf_serve.cu", "ffbf_static.cu", "ffbf_hashbench.cu"]
+CUDA_SOURCES = ["ffbf_kernels.cu", "ffbf_scan_fast.cu", "ffbf_capi.cu", "ffbf_batch.cu", "ffbf_serve.cu", "ffbf_static.cu", "ffbf_hashbench.cu", "ffbf_order.cu"]
 
 
 def _newer(target, deps):

@@ -21,6 +21,7 @@
 #include "ffbf_scan_fast.cuh"
 
 #include "ffbf_ctx.cuh"
+#include "ffbf_order.cuh"
 
 using ffbf::Geom;
 using ffbf::HitLine;
@@ -64,6 +65,16 @@ ffbf_status ensure_tmp(ffbf_ctx* c, size_t words) {
     c->tmp_words = 0;
     TRY(dalloc_t(c, &c->d_tmp, words));
     c->tmp_words = words;
+    return FFBF_OK;
+}
+
+// Grows the result-ordering scratch to at least `bytes`.
+ffbf_status ensure_order(ffbf_ctx* c, size_t bytes) {
+    if (c->order_bytes >= bytes) return FFBF_OK;
+    dfree(c, c->d_order);
+    c->order_bytes = 0;
+    TRY(dalloc_t(c, &c->d_order, bytes));
+    c->order_bytes = bytes;
     return FFBF_OK;
 }
 
@@ -696,16 +707,42 @@ ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
                                         c->d_tiles + c->tiles_cap, c->d_tiles + 2 * c->tiles_cap,
                                         c->d_tiles + 3 * c->tiles_cap, ntiles, c->d_hitlines, c->st,
                                         c->d_tiles + 4 * c->tiles_cap));
-        std::vector<HitRec> hr(nh);
-        std::vector<HitLine> hl(nh);
-        if (nh) {
+        // text order on the device: sorted window starts, then the distinct lines of the sorted windows
+        const int kb = ffbf::key_bits_for(c->text_len);
+        const size_t scratch = ffbf::order_hits_scratch(nh, kb);
+        const size_t off_bytes = ((size_t)nh * 8 + 255) / 256 * 256, line_bytes = ((size_t)nh * 16 + 255) / 256 * 256;
+        TRY(ensure_order(c, off_bytes + line_bytes + 256 + scratch));
+        uint64_t* d_off = reinterpret_cast<uint64_t*>(c->d_order);
+        HitLine* d_lu = reinterpret_cast<HitLine*>(c->d_order + off_bytes);
+        uint64_t* d_nl = reinterpret_cast<uint64_t*>(c->d_order + off_bytes + line_bytes);
+        CUDA_TRY(c, ffbf::order_hits(c->d_hits, c->d_hitlines, nh, kb, c->d_order + off_bytes + line_bytes + 256,
+                                     scratch, d_off, d_lu, d_nl, c->st));
+        if (c->keep_records && nh) {
+            // a segment of a larger text: ffbf_verify needs its records again
+            std::vector<HitRec> hr(nh);
             CUDA_TRY(c, cudaMemcpyAsync(hr.data(), c->d_hits, nh * sizeof(HitRec), cudaMemcpyDeviceToHost, c->st));
-            CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->d_hitlines, nh * sizeof(HitLine), cudaMemcpyDeviceToHost, c->st));
-        }
-        TRY(sync(c));
-        if (c->keep_records)  // a segment of a larger text: ffbf_verify needs its records again
+            TRY(sync(c));
             for (uint32_t i = 0; i < nh; i++) c->seg_hr.push_back(HitRec{hr[i].off + c->seg_base, hr[i].h});
-        order_hits(hr.data(), hl.data(), nh, c->r_hits, c->r_ls, c->r_le);
+        }
+        uint64_t n_lines = 0;
+        c->r_hits.resize(nh);
+        if (nh)
+            CUDA_TRY(c, cudaMemcpyAsync(c->r_hits.data(), d_off, nh * 8ull, cudaMemcpyDeviceToHost, c->st));
+        CUDA_TRY(c, cudaMemcpyAsync(&n_lines, d_nl, 8, cudaMemcpyDeviceToHost, c->st));
+        TRY(sync(c));
+        if (n_lines > nh) return fail(c, FFBF_ECUDA, "line reduction returned %llu lines for %u hits",
+                                      (unsigned long long)n_lines, nh);
+        std::vector<HitLine> lines(n_lines);
+        if (n_lines) {
+            CUDA_TRY(c, cudaMemcpyAsync(lines.data(), d_lu, n_lines * sizeof(HitLine), cudaMemcpyDeviceToHost, c->st));
+            TRY(sync(c));
+        }
+        c->r_ls.resize(n_lines);
+        c->r_le.resize(n_lines);
+        for (uint64_t i = 0; i < n_lines; i++) {
+            c->r_ls[i] = lines[i].start;
+            c->r_le[i] = lines[i].end;
+        }
         c->scan_pending = false;
         c->have_scan = true;
     }
@@ -965,8 +1002,14 @@ ffbf_status ffbf_prune(ffbf_ctx* c, ffbf_prune_result* out) {
     const uint64_t n = c->npat;
     const uint64_t nb = ffbf::compact_blocks(n);
     TRY(ensure_tmp(c, nb + 1));
-    uint8_t* d_flags = nullptr;
-    TRY(dalloc_t(c, &d_flags, n + 1));
+    // the flags and id buffers are kept between calls: a cudaFree would wait for the whole device
+    if (c->pflags_cap < n + 1) {
+        dfree(c, c->d_pflags);
+        c->pflags_cap = 0;
+        TRY(dalloc_t(c, &c->d_pflags, n + 1));
+        c->pflags_cap = n + 1;
+    }
+    uint8_t* d_flags = c->d_pflags;
     ffbf_status s = FFBF_OK;
     uint64_t cnt = 0;
     if (ffbf::prune_flags(c->d_pstart, c->d_pend, c->d_phash, n, c->g, c->d_ff, d_flags, c->st) != cudaSuccess ||
@@ -974,9 +1017,11 @@ ffbf_status ffbf_prune(ffbf_ctx* c, ffbf_prune_result* out) {
         cudaMemcpyAsync(&cnt, c->d_tmp + nb, 8, cudaMemcpyDeviceToHost, c->st) != cudaSuccess ||
         cudaStreamSynchronize(c->st) != cudaSuccess)
         s = fail(c, FFBF_ECUDA, "prune failed: %s", cudaGetErrorString(cudaGetLastError()));
-    if (s == FFBF_OK) {
+    if (s == FFBF_OK && c->ids_cap < cnt + 1) {
         dfree(c, c->d_ids);
+        c->ids_cap = 0;
         s = dalloc_t(c, &c->d_ids, cnt + 1);
+        if (s == FFBF_OK) c->ids_cap = cnt + 1;
     }
     if (s == FFBF_OK) {
         c->r_ids.resize(cnt);
@@ -985,7 +1030,6 @@ ffbf_status ffbf_prune(ffbf_ctx* c, ffbf_prune_result* out) {
             cudaStreamSynchronize(c->st) != cudaSuccess)
             s = fail(c, FFBF_ECUDA, "prune compaction failed: %s", cudaGetErrorString(cudaGetLastError()));
     }
-    dfree(c, d_flags);
     if (s != FFBF_OK) return s;
     c->nids = cnt;
     c->have_prune = true;
@@ -1063,6 +1107,11 @@ ffbf_status verify_pass(ffbf_ctx* c, uint32_t nh, const uint8_t* d_text, uint64_
         c->match_cap = (uint32_t)cap;
     }
     const uint32_t nm = c->h_counters[ffbf::CNT_MATCHES];
+    // (offset, pattern id) order on the device
+    const int kb = ffbf::key_bits_for(text_len);
+    const size_t scratch = ffbf::order_matches_scratch(nm, kb);
+    TRY(ensure_order(c, scratch));
+    CUDA_TRY(c, ffbf::order_matches(c->d_moff, c->d_mpid, nm, kb, c->d_order, scratch, c->st));
     const size_t at = off_out.size();
     off_out.resize(at + nm);
     pid_out.resize(at + nm);
@@ -1131,18 +1180,11 @@ ffbf_status ffbf_verify(ffbf_ctx* c, ffbf_matches* out) {
             TRY(verify_pass(c, (uint32_t)nh, c->d_text_own, sg.len, tsize, sg.pos, off, pid));
         }
     }
+    // each pass's matches come sorted, and segments follow one another in the text
     const size_t nm = off.size();
-    std::vector<uint32_t> order(nm);
-    for (uint32_t i = 0; i < nm; i++) order[i] = i;
-    std::sort(order.begin(), order.end(), [&](uint32_t a, uint32_t b) {
-        return off[a] != off[b] ? off[a] < off[b] : pid[a] < pid[b];
-    });
-    c->r_moff.resize(nm);
+    c->r_moff.swap(off);
     c->r_mpid.resize(nm);
-    for (uint32_t i = 0; i < nm; i++) {
-        c->r_moff[i] = off[order[i]];
-        c->r_mpid[i] = pid[order[i]];
-    }
+    for (size_t i = 0; i < nm; i++) c->r_mpid[i] = pid[i];
     if (out) {
         out->n = nm;
         out->offsets = c->r_moff.data();

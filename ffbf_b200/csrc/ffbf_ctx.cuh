@@ -118,6 +118,11 @@ struct ffbf_ctx {
     // scratch for ordered compaction / codec
     uint64_t* d_tmp = nullptr;
     size_t tmp_words = 0;
+    // scratch of the result ordering (sorts and selections), and the prune's per-pattern flags
+    uint8_t* d_order = nullptr;
+    size_t order_bytes = 0;
+    uint8_t* d_pflags = nullptr;
+    uint64_t pflags_cap = 0, ids_cap = 0;
     uint8_t* d_small = nullptr;  // test_line input
     size_t small_cap = 0;
 };
