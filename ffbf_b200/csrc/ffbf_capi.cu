@@ -761,11 +761,19 @@ ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
 
 namespace {
 
-constexpr uint64_t kPipeChunk = 128ull << 20;  // bytes per overlapped copy of a host text
+// Host texts of kPipeMinText bytes or more are copied in chunks that the scan follows; a chunk is about an
+// eighth of the text, between 8 and 128 MiB.
+constexpr uint64_t kPipeMinText = 32ull << 20;
+constexpr uint64_t kPipeChunkMin = 8ull << 20, kPipeChunkMax = 128ull << 20;
+
+uint64_t pipe_chunk(uint64_t len) {
+    return std::min(kPipeChunkMax, std::max(kPipeChunkMin, len / 8 >> 20 << 20));
+}
 
 // The scan of a host text whose copy to the device overlaps the scan: the text goes over in chunks of
-// about kPipeChunk bytes on the context's copy stream, and after each chunk the tuned kernel runs over
-// the work items whose bytes (and halos) have landed. Every chunk's launch uses the whole text's tensor
+// about pipe_chunk(len) bytes on the context's copy stream, and after each chunk the tuned kernel runs over
+// the work items whose bytes (and halos) have landed. The rows per stream suit one chunk, whose launch
+// then spreads over the SMs and ends soon after its copy; the copy is the bound. Every chunk's launch uses the whole text's tensor
 // map and absolute positions; its descriptor only shifts the item numbering (item_begin = -first item).
 ffbf_status scan_host_pipelined(ffbf_ctx* c, const uint8_t* text, size_t len) {
     TRY(setup_scan_state(c, c->d_text_own, len));
@@ -774,13 +782,14 @@ ffbf_status scan_host_pipelined(ffbf_ctx* c, const uint8_t* text, size_t len) {
     c->scan_path = 1;
     const ffbf::ScanArgs a = make_scan_args(c);
     const int threads = ffbf::config_threads(c->cfg);
-    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(len, c->cfg, c->num_sms, false);
+    const uint64_t chunk = pipe_chunk(len);
+    const uint32_t rows = c->cfg.rows ? c->cfg.rows : ffbf::fast_rows(chunk, c->cfg, c->num_sms, false);
     ffbf::FastJob job;
     cudaError_t e;
     const uint64_t covered = ffbf::fill_fast_job(a, c->d_stage1, c->cfg, rows, &job, &e);
     if (e != cudaSuccess) return fail(c, FFBF_ECUDA, "tensor map encoding failed");
     const uint64_t item_bytes = (uint64_t)threads * rows * 128;
-    const uint32_t per_chunk = (uint32_t)std::max<uint64_t>(1, kPipeChunk / item_bytes);
+    const uint32_t per_chunk = (uint32_t)std::max<uint64_t>(1, chunk / item_bytes);
     const uint32_t n_chunks = (job.n_supertiles + per_chunk - 1) / per_chunk;
     if (!c->st_copy) CUDA_TRY(c, cudaStreamCreateWithFlags(&c->st_copy, cudaStreamNonBlocking));
     while (c->pipe_events.size() < (size_t)n_chunks + 2) {
@@ -854,7 +863,7 @@ ffbf_status scan_one(ffbf_ctx* c, const uint8_t* text, size_t len, ffbf_scan_res
         TRY(dalloc_t(c, &c->d_text_own, len + 64));
         c->text_cap = len + 64;
     }
-    if (len >= 2 * kPipeChunk && use_fast(c, len)) {
+    if (len >= kPipeMinText && use_fast(c, len)) {
         TRY(scan_host_pipelined(c, text, len));
         c->scan_pending = true;
         return ffbf_scan_collect(c, out);

@@ -114,7 +114,7 @@ typedef struct {
  * and is not hashed); every window whose K main bits are set marks its line and sets K bits of the
  * feed-forward filter in getHashValue_2 order (ffbf.cpp:161-185). The feed-forward filter accumulates
  * over successive scans, as it does over one reference run; ffbf_clear_ff starts a new one.
- * A text of 256 MiB or more is copied in chunks while the chunks already on the device are scanned. A text
+ * A text of 32 MiB or more is copied in chunks while the chunks already on the device are scanned. A text
  * larger than the device can hold (its free memory, or the context's HBM budget) is scanned in segments
  * that each end after a '\n' (a line longer than a segment gives FFBF_EINVAL); the results are the same,
  * and ffbf_verify then copies the segments again, so the text must stay valid until ffbf_verify. */

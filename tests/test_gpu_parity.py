@@ -289,20 +289,24 @@ def test_line_resolution_over_many_tile_blocks():
         np.testing.assert_array_equal(f.get_filters()[1], o.ff)
 
 
-def test_host_text_scan_with_overlapped_copy_equals_oracle():
-    """A host text of at least two 128 MiB chunks is copied in chunks while the scan runs on the chunks that
-    have landed; windows, lines and the feed-forward filter equal the oracle's, including windows and a
-    50 MiB line across chunk boundaries."""
+@pytest.mark.parametrize("mib", [300, 40])
+def test_host_text_scan_with_overlapped_copy_equals_oracle(mib):
+    """A host text of 32 MiB or more is copied in chunks (about an eighth of the text, 8-128 MiB) while the
+    scan runs on the chunks that have landed; windows, lines and the feed-forward filter equal the oracle's,
+    including windows across every MiB boundary (chunk boundaries fall on whole MiB here) and a long line
+    across chunks."""
     from ffbf_b200 import datagen as dg
 
     prm = Params(20, 5, 2, 1 << 24, 1 << 28)
     pats = dg.gen_patterns(41, dg.PRINTABLE, 3000, 20, 40)
-    text = dg.gen_text(42, dg.PRINTABLE, 300 << 20, 2000)
-    seg = text[(100 << 20) - 1000:(150 << 20)]
+    text = dg.gen_text(42, dg.PRINTABLE, mib << 20, 2000)
+    lo, hi = (mib << 20) // 3, (mib << 20) // 2
+    seg = text[lo:hi]
     seg[seg == 10] = ord("y")
     dg.plant(43, pats, text, 4000)
-    for k in range(1, 3):  # occurrences straddling the first chunk boundaries
-        text[(k << 27) - 10:(k << 27) - 10 + 25] = np.frombuffer(pats[:25].tobytes(), dtype=np.uint8)
+    occ = np.frombuffer(pats[:25].tobytes(), dtype=np.uint8)
+    for k in range(1, mib):  # occurrences straddling each MiB boundary
+        text[(k << 20) - 10:(k << 20) - 10 + occ.size] = occ
     o = oracle.Oracle.from_params(prm)
     o.build(pats)
     s = o.scan(text)
@@ -313,6 +317,7 @@ def test_host_text_scan_with_overlapped_copy_equals_oracle():
         np.testing.assert_array_equal(r.line_start, s["line_start"])
         np.testing.assert_array_equal(r.line_end, s["line_end"])
         np.testing.assert_array_equal(f.get_filters()[1], o.ff)
+    assert any((k << 20) - 10 in set(s["hits"].tolist()) for k in range(1, 4)), "a straddling window should hit"
 
 
 def test_text_larger_than_the_device_budget_is_scanned_in_segments():
