@@ -402,6 +402,8 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
     if (fo && fo[0] >= '0' && fo[0] <= '2') c->force_order = fo[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");
     c->force_generic = fg && fg[0] == '1';
+    const char* ho = getenv("FFBF_HOST_ORDER");
+    c->host_order = ho && ho[0] == '1';
     *out = c;
     return FFBF_OK;
 }
@@ -707,41 +709,55 @@ ffbf_status ffbf_scan_collect(ffbf_ctx* c, ffbf_scan_result* out) {
                                         c->d_tiles + c->tiles_cap, c->d_tiles + 2 * c->tiles_cap,
                                         c->d_tiles + 3 * c->tiles_cap, ntiles, c->d_hitlines, c->st,
                                         c->d_tiles + 4 * c->tiles_cap));
-        // text order on the device: sorted window starts, then the distinct lines of the sorted windows
+        // Text order on the device: sorted window starts, then the distinct lines of the sorted windows. When
+        // the device has no room for the sort's scratch (about 60 bytes per hit window), or FFBF_HOST_ORDER is
+        // set, the records are ordered on the host instead; the results are the same.
         const int kb = ffbf::key_bits_for(c->text_len);
         const size_t scratch = ffbf::order_hits_scratch(nh, kb);
         const size_t off_bytes = ((size_t)nh * 8 + 255) / 256 * 256, line_bytes = ((size_t)nh * 16 + 255) / 256 * 256;
-        TRY(ensure_order(c, off_bytes + line_bytes + 256 + scratch));
-        uint64_t* d_off = reinterpret_cast<uint64_t*>(c->d_order);
-        HitLine* d_lu = reinterpret_cast<HitLine*>(c->d_order + off_bytes);
-        uint64_t* d_nl = reinterpret_cast<uint64_t*>(c->d_order + off_bytes + line_bytes);
-        CUDA_TRY(c, ffbf::order_hits(c->d_hits, c->d_hitlines, nh, kb, c->d_order + off_bytes + line_bytes + 256,
-                                     scratch, d_off, d_lu, d_nl, c->st));
-        if (c->keep_records && nh) {
-            // a segment of a larger text: ffbf_verify needs its records again
-            std::vector<HitRec> hr(nh);
+        const bool on_device = !c->host_order && ensure_order(c, off_bytes + line_bytes + 256 + scratch) == FFBF_OK;
+        if (!on_device) c->err.clear();
+        std::vector<HitRec> hr;
+        if (nh && (c->keep_records || !on_device)) {
+            hr.resize(nh);
             CUDA_TRY(c, cudaMemcpyAsync(hr.data(), c->d_hits, nh * sizeof(HitRec), cudaMemcpyDeviceToHost, c->st));
             TRY(sync(c));
+        }
+        if (c->keep_records)  // a segment of a larger text: ffbf_verify needs its records again
             for (uint32_t i = 0; i < nh; i++) c->seg_hr.push_back(HitRec{hr[i].off + c->seg_base, hr[i].h});
-        }
-        uint64_t n_lines = 0;
-        c->r_hits.resize(nh);
-        if (nh)
-            CUDA_TRY(c, cudaMemcpyAsync(c->r_hits.data(), d_off, nh * 8ull, cudaMemcpyDeviceToHost, c->st));
-        CUDA_TRY(c, cudaMemcpyAsync(&n_lines, d_nl, 8, cudaMemcpyDeviceToHost, c->st));
-        TRY(sync(c));
-        if (n_lines > nh) return fail(c, FFBF_ECUDA, "line reduction returned %llu lines for %u hits",
-                                      (unsigned long long)n_lines, nh);
-        std::vector<HitLine> lines(n_lines);
-        if (n_lines) {
-            CUDA_TRY(c, cudaMemcpyAsync(lines.data(), d_lu, n_lines * sizeof(HitLine), cudaMemcpyDeviceToHost, c->st));
+        if (!on_device) {
+            std::vector<HitLine> hl(nh);
+            if (nh)
+                CUDA_TRY(c, cudaMemcpyAsync(hl.data(), c->d_hitlines, nh * sizeof(HitLine), cudaMemcpyDeviceToHost,
+                                            c->st));
             TRY(sync(c));
-        }
-        c->r_ls.resize(n_lines);
-        c->r_le.resize(n_lines);
-        for (uint64_t i = 0; i < n_lines; i++) {
-            c->r_ls[i] = lines[i].start;
-            c->r_le[i] = lines[i].end;
+            order_hits(hr.data(), hl.data(), nh, c->r_hits, c->r_ls, c->r_le);
+        } else {
+            uint64_t* d_off = reinterpret_cast<uint64_t*>(c->d_order);
+            HitLine* d_lu = reinterpret_cast<HitLine*>(c->d_order + off_bytes);
+            uint64_t* d_nl = reinterpret_cast<uint64_t*>(c->d_order + off_bytes + line_bytes);
+            CUDA_TRY(c, ffbf::order_hits(c->d_hits, c->d_hitlines, nh, kb, c->d_order + off_bytes + line_bytes + 256,
+                                         scratch, d_off, d_lu, d_nl, c->st));
+            uint64_t n_lines = 0;
+            c->r_hits.resize(nh);
+            if (nh)
+                CUDA_TRY(c, cudaMemcpyAsync(c->r_hits.data(), d_off, nh * 8ull, cudaMemcpyDeviceToHost, c->st));
+            CUDA_TRY(c, cudaMemcpyAsync(&n_lines, d_nl, 8, cudaMemcpyDeviceToHost, c->st));
+            TRY(sync(c));
+            if (n_lines > nh) return fail(c, FFBF_ECUDA, "line reduction returned %llu lines for %u hits",
+                                          (unsigned long long)n_lines, nh);
+            std::vector<HitLine> lines(n_lines);
+            if (n_lines) {
+                CUDA_TRY(c, cudaMemcpyAsync(lines.data(), d_lu, n_lines * sizeof(HitLine), cudaMemcpyDeviceToHost,
+                                            c->st));
+                TRY(sync(c));
+            }
+            c->r_ls.resize(n_lines);
+            c->r_le.resize(n_lines);
+            for (uint64_t i = 0; i < n_lines; i++) {
+                c->r_ls[i] = lines[i].start;
+                c->r_le[i] = lines[i].end;
+            }
         }
         c->scan_pending = false;
         c->have_scan = true;
@@ -773,8 +789,9 @@ uint64_t pipe_chunk(uint64_t len) {
 // The scan of a host text whose copy to the device overlaps the scan: the text goes over in chunks of
 // about pipe_chunk(len) bytes on the context's copy stream, and after each chunk the tuned kernel runs over
 // the work items whose bytes (and halos) have landed. The rows per stream suit one chunk, whose launch
-// then spreads over the SMs and ends soon after its copy; the copy is the bound. Every chunk's launch uses the whole text's tensor
-// map and absolute positions; its descriptor only shifts the item numbering (item_begin = -first item).
+// then spreads over the SMs and ends soon after its copy; the copy is the bound. Every chunk's launch uses
+// the whole text's tensor map and absolute positions; its descriptor only shifts the item numbering
+// (item_begin = -first item).
 ffbf_status scan_host_pipelined(ffbf_ctx* c, const uint8_t* text, size_t len) {
     TRY(setup_scan_state(c, c->d_text_own, len));
     CUDA_TRY(c, cudaMemsetAsync(c->d_counters, 0, ffbf::CNT_WORDS * sizeof(uint32_t), c->st));
@@ -1116,11 +1133,12 @@ ffbf_status verify_pass(ffbf_ctx* c, uint32_t nh, const uint8_t* d_text, uint64_
         c->match_cap = (uint32_t)cap;
     }
     const uint32_t nm = c->h_counters[ffbf::CNT_MATCHES];
-    // (offset, pattern id) order on the device
+    // (offset, pattern id) order on the device, or on the host as the hits' order is (see ffbf_scan_collect)
     const int kb = ffbf::key_bits_for(text_len);
     const size_t scratch = ffbf::order_matches_scratch(nm, kb);
-    TRY(ensure_order(c, scratch));
-    CUDA_TRY(c, ffbf::order_matches(c->d_moff, c->d_mpid, nm, kb, c->d_order, scratch, c->st));
+    const bool on_device = !c->host_order && ensure_order(c, scratch) == FFBF_OK;
+    if (!on_device) c->err.clear();
+    if (on_device) CUDA_TRY(c, ffbf::order_matches(c->d_moff, c->d_mpid, nm, kb, c->d_order, scratch, c->st));
     const size_t at = off_out.size();
     off_out.resize(at + nm);
     pid_out.resize(at + nm);
@@ -1129,6 +1147,15 @@ ffbf_status verify_pass(ffbf_ctx* c, uint32_t nh, const uint8_t* d_text, uint64_
         CUDA_TRY(c, cudaMemcpyAsync(pid_out.data() + at, c->d_mpid, nm * 4ull, cudaMemcpyDeviceToHost, c->st));
     }
     TRY(sync(c));
+    if (!on_device) {
+        std::vector<std::pair<uint64_t, uint32_t>> m(nm);
+        for (size_t i = 0; i < nm; i++) m[i] = {off_out[at + i], pid_out[at + i]};
+        std::sort(m.begin(), m.end());
+        for (size_t i = 0; i < nm; i++) {
+            off_out[at + i] = m[i].first;
+            pid_out[at + i] = m[i].second;
+        }
+    }
     for (size_t i = at; i < off_out.size(); i++) off_out[i] += base;
     return FFBF_OK;
 }

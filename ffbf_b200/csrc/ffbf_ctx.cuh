@@ -123,6 +123,7 @@ struct ffbf_ctx {
     size_t order_bytes = 0;
     uint8_t* d_pflags = nullptr;
     uint64_t pflags_cap = 0, ids_cap = 0;
+    bool host_order = false;  // FFBF_HOST_ORDER: order results on the host (a check of the device ordering)
     uint8_t* d_small = nullptr;  // test_line input
     size_t small_cap = 0;
 };

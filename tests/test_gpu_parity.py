@@ -219,6 +219,29 @@ def test_scan_variants_agree_with_oracle(name, monkeypatch):
         pass  # restores the default CTA size for later tests
 
 
+@pytest.mark.parametrize("name", ["hit_flood", "edge_mixed", "binary_small", "scale_small", "empty_text"])
+def test_device_and_host_result_order_agree(name, monkeypatch):
+    """Scan results and verified matches are put in text order on the device (radix sorts and a line
+    selection); FFBF_HOST_ORDER=1 orders the same records on the host, the path taken when the device has no
+    room for the sort. Both give the oracle's hit windows, lines and (offset, pattern id) matches, including
+    many hits per line (hit_flood) and one offset matched by several pattern ids (edge_mixed)."""
+    prm, pats, text = build_inputs(name)
+    o, s, pr, ooff, opid = run_oracle(prm, pats, text)
+    for host in ("0", "1"):
+        monkeypatch.setenv("FFBF_HOST_ORDER", host)
+        with Filter(prm) as f:
+            f.add_patterns(pats)
+            r = f.process(text)
+            np.testing.assert_array_equal(r.hit_offsets, s["hits"], err_msg=host)
+            np.testing.assert_array_equal(r.line_start, s["line_start"], err_msg=host)
+            np.testing.assert_array_equal(r.line_end, s["line_end"], err_msg=host)
+            np.testing.assert_array_equal(f.filter_phrases(), pr["ids"], err_msg=host)
+            off, pid = f.verify()
+            np.testing.assert_array_equal(off, ooff, err_msg=host)
+            np.testing.assert_array_equal(pid, opid, err_msg=host)
+    monkeypatch.delenv("FFBF_HOST_ORDER", raising=False)
+
+
 @pytest.mark.parametrize("L,k,s", [(20, 1, 1), (20, 2, 1), (20, 2, 2), (24, 3, 1), (24, 4, 3), (24, 4, 4),
                                    (32, 5, 1), (16, 6, 2), (19, 11, 0)])
 def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
