@@ -495,7 +495,8 @@ def run_batched(args, local):
         "autotune_classes": n_classes,
         "configs": dict(collections.Counter(
             (f"dense-{f.config()[0]}-order{f.probe_order()}" if f.config()[1] == 1 else
-             f"sparse-deferred-{f.config()[0]}" if f.config()[1] == 2 else f"sparse-{f.config()[0]}")
+             f"sparse-deferred-{f.config()[0]}" if f.config()[1] == 2 else
+             f"sparse-staged-{f.config()[0]}" if f.config()[1] == 3 else f"sparse-{f.config()[0]}")
             for f in filters)),
         "timing": "host clock between device-idle points, median of steps; batched_device = CUDA events",
         "lone_jobs_without_gaps": ideal,

@@ -417,11 +417,12 @@ ffbf_status autotune_impl(ffbf_ctx* c, const uint8_t* d_text, size_t sample_len,
     uint32_t* saved = nullptr;
     TRY(dalloc_t(c, &saved, c->filter_bytes / 4));
     CUDA_TRY(c, cudaMemcpyAsync(saved, c->d_ff, c->filter_bytes, cudaMemcpyDeviceToDevice, c->st));
-    // shared-memory mode at three CTA sizes with candidates queued per byte and at two with candidates
-    // deferred to the end of each block, dense mode at three (its probe order follows the filter's fills;
-    // 192 runs two CTAs per SM, and probe order 2 runs 192 as 384)
-    const ffbf::FastConfig cands[] = {{512, 0, 0, 0}, {384, 0, 0, 0}, {256, 0, 0, 0}, {256, 2, 0, 0},
-                                      {192, 2, 0, 0}, {384, 1, 0, 0}, {192, 1, 0, 0}, {256, 1, 0, 0}};
+    // shared-memory mode at three CTA sizes with candidates queued per byte (512 also with per-stage
+    // barriers) and at two with candidates deferred to the end of each block, dense mode at three (its probe
+    // order follows the filter's fills; 192 runs two CTAs per SM, and probe order 2 runs 192 as 384)
+    const ffbf::FastConfig cands[] = {{512, 0, 0, 0}, {512, 3, 0, 0}, {384, 0, 0, 0}, {256, 0, 0, 0},
+                                      {256, 2, 0, 0}, {192, 2, 0, 0}, {384, 1, 0, 0}, {192, 1, 0, 0},
+                                      {256, 1, 0, 0}};
     ffbf::FastConfig best = c->cfg;
     double best_score = 1e300;
     cudaEvent_t e0, e1;

@@ -217,7 +217,10 @@ ffbf_status prepare_fast(ffbf_ctx* c) {
         c->stage1_fill = (double)ones[0] / (32.0 * c->stage1_words);
         c->probe_order = ffbf::dense_probe_order(c->g, (double)ones[1] / (32.0 * cw), (double)ones[2] / (32.0 * ew));
         if (!c->cfg_tuned) {
-            c->cfg.mode = c->force_mode >= 0 ? c->force_mode : c->stage1_fill > 0.3 ? 1 : 0;
+            // the shared-memory stage passes about fill^2 of the windows (fill with S = 1); below 1 % the
+            // warps rarely queue candidates and run apart through per-stage barriers (mode 3)
+            const double pass = c->g.s > 1 ? c->stage1_fill * c->stage1_fill : c->stage1_fill;
+            c->cfg.mode = c->force_mode >= 0 ? c->force_mode : c->stage1_fill > 0.3 ? 1 : pass < 0.01 ? 3 : 0;
             // default CTA sizes (measured best on the 10k- and 1M-pattern workloads): 512 threads for the
             // shared-memory stage, 2 x 192 per SM for dense filters
             // (dense: two 192-thread CTAs per SM; probe order 2 needs the 384-thread CTA's room for its table)
@@ -397,7 +400,7 @@ ffbf_status ffbf_create(const ffbf_params* p, int device, ffbf_ctx** out) {
     if (th && (atoi(th) == 192 || atoi(th) == 256 || atoi(th) == 384 || atoi(th) == 512))
         c->cfg.threads = c->threads_env = atoi(th);
     const char* fm = getenv("FFBF_SCAN_MODE");
-    if (fm && fm[0] >= '0' && fm[0] <= '2') c->force_mode = fm[0] - '0';
+    if (fm && fm[0] >= '0' && fm[0] <= '3') c->force_mode = fm[0] - '0';
     const char* fo = getenv("FFBF_SCAN_ORDER");
     if (fo && fo[0] >= '0' && fo[0] <= '2') c->force_order = fo[0] - '0';
     const char* fg = getenv("FFBF_FORCE_GENERIC_SCAN");

@@ -55,6 +55,13 @@ __device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
     asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(bar), "r"(count) : "memory");
 }
 
+__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
+    asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(bar) : "memory");
+}
+
+// Waits for the phase of the given parity, at most kWaitLimit polls; false when it gave up.
+__device__ __noinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity);
+
 __device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
     asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(bar), "r"(bytes) : "memory");
 }
@@ -69,6 +76,12 @@ __device__ __forceinline__ bool mbar_try_wait(uint32_t bar, uint32_t parity) {
         : "r"(bar), "r"(parity)
         : "memory");
     return ok != 0;
+}
+
+__device__ __noinline__ bool mbar_wait_bounded(uint32_t bar, uint32_t parity) {
+    for (uint32_t it = 0; it < kWaitLimit; it++)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
 }
 
 __device__ __forceinline__ void tma_load_3d(uint32_t dst, const CUtensorMap* map, int x, int y, int z, uint32_t bar) {
@@ -95,8 +108,8 @@ __device__ __forceinline__ uint64_t l2_evict_first_policy() {
     return p;
 }
 
-// Shared-memory loads the compiler may schedule freely (the tables are read-only after set-up, and every
-// later write to the stages is ordered by __syncthreads).
+// Shared-memory loads of the read-only tables, which the compiler may schedule freely (a table is
+// rewritten only between block barriers, at a change of job).
 __device__ __forceinline__ uint2 lds64(uint32_t addr) {
     uint2 v;
     asm("ld.shared.v2.u32 {%0, %1}, [%2];" : "=r"(v.x), "=r"(v.y) : "r"(addr));
@@ -286,6 +299,8 @@ __device__ __forceinline__ uint32_t newline_mask32(const uint32_t (&w)[8]) {
 // CTAs per SM: the dense modes at 192 threads run two CTAs per SM (12 warps, as one 384-thread CTA, but two
 // independent pipelines and barriers of 6 warps each); every other configuration runs one.
 __host__ __device__ constexpr int ctas_per_sm(int threads, int mode) { return threads == 192 && mode >= 1 && mode <= 3 ? 2 : 1; }
+// MODE 5 is MODE 0 whose warps meet through per-stage barriers instead of a block barrier per stage
+__host__ __device__ constexpr bool sparse_mode(int mode) { return mode == 0 || mode == 5; }
 
 template <int L, int THREADS, int MODE>
 __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fast(const FastJob* __restrict__ jobs, uint32_t n_jobs,
@@ -294,13 +309,14 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
     // ctl[0]: error flags; ctl[1]: the work queue, the count of items handed out past the first wave
     uint32_t* const error_flag = ctl;
     constexpr int kStageBytes = THREADS * kRowBytes;
-    constexpr int kQCap = (MODE == 0 || MODE == 4) ? kQueueCap : 2 * kQueueCap;
+    constexpr int kQCap = (sparse_mode(MODE) || MODE == 4) ? kQueueCap : 2 * kQueueCap;
     constexpr int kQBytes = kQCap * 16;
     // dense mode: ring depth per stage (divides 32); 384-thread CTAs trade depth for warps (more L2 probes
     // in flight per SM within the register file)
     constexpr int kRing = THREADS >= 384 || ctas_per_sm(THREADS, MODE) == 2 ? 4 : 8;
     constexpr int kBox = THREADS > 256 ? THREADS / 2 : THREADS;  // streams per TMA box (<= 256)
-    constexpr bool kTable = MODE == 0 || MODE == 3 || MODE == 4;  // reads the stage-1 table
+    constexpr bool kTable = sparse_mode(MODE) || MODE == 3 || MODE == 4;  // reads the stage-1 table
+    constexpr bool kSparse = sparse_mode(MODE);
     extern __shared__ uint8_t smem_raw[];
     const uint32_t raw = smem_u32(smem_raw);
     const uint32_t base = (raw + 1023u) & ~1023u;
@@ -309,6 +325,14 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
     const uint32_t stage0 = base;
     const uint32_t tab = base + 2 * kStageBytes;
     const uint32_t bar0 = tab + kTabBytes, bar1 = bar0 + 8;
+    // Stage k & 1's "full" barrier completes when load k lands. With kStageBarriers (MODE 5) its "empty"
+    // barrier completes when every warp is done reading it, load k + 2 reuses the stage only after that, and
+    // warps otherwise run apart by up to a stage. It pays where few windows pass the shared-memory stage
+    // (plain workload: 596 -> 630 GB/s); where many do, warps that wait for the stage of a warp busy with
+    // its queue cost more than a block barrier (a 2^22-bit batched class: 370 -> 306), and in the dense
+    // modes too (325 -> 308). The other modes keep one block barrier per stage.
+    constexpr bool kStageBarriers = MODE == 5;
+    auto ebar = [&](uint32_t k) { return bar0 + 48u + 8u * (k & 1u); };
     int* meta = reinterpret_cast<int*>(smem + 2 * kStageBytes + kTabBytes + 16);  // [buf][4]: job, item, row, valid
     const uint32_t queues = bar0 + 128;
     const uint32_t s1 = queues + (THREADS / 32) * kQBytes;
@@ -330,14 +354,23 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
             tp[i] = c_sbox[(c & 0x80) ? 0 : c];
         }
     }
-    // load sequencer, run by thread 0: the next load is row nr (-1: halo) of item ni, which belongs to job nj
-    auto issue = [&](uint32_t k) {
+    // load sequencer, run by thread 0: the next load is row nr (-1: halo) of item ni, which belongs to job nj.
+    // Load k waits (bounded) until every warp has released load k - 2's stage; with no item left it completes
+    // the stage's full barrier without a load and marks the end in meta. Returns false when the wait gave up.
+    auto issue = [&](uint32_t k) -> bool {
+        if constexpr (kStageBarriers) {
+            if (k >= 2 && !mbar_wait_bounded(ebar(k), ((k - 2) >> 1) & 1u)) {
+                atomicOr(error_flag, 4u);
+                return false;
+            }
+        }
         int* m = meta + 4 * (k & 1);
         uint32_t ni = s_ni, nj = s_nj;
         int nr = s_nr;
         if (ni >= n_items) {
             m[3] = 0;
-            return;
+            if constexpr (kStageBarriers) mbar_arrive((k & 1) ? bar1 : bar0);
+            return true;
         }
         while (nj + 1 < n_jobs && __ldg(&jobs[nj + 1].item_begin) <= ni) nj++;
         const FastJob* J = jobs + nj;
@@ -367,6 +400,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
         s_ni = ni;
         s_nj = nj;
         s_nr = nr;
+        return true;
     };
     if (tid == 0) {
         s_abort = 0;
@@ -375,6 +409,10 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
         s_nr = -1;
         mbar_init(bar0, 1);
         mbar_init(bar1, 1);
+        if constexpr (kStageBarriers) {
+            mbar_init(ebar(0), THREADS / 32);
+            mbar_init(ebar(1), THREADS / 32);
+        }
         *reinterpret_cast<uint32_t*>(smem + (bar0 - base) + 64) = 0xFFFFFFFFu;  // the S = 1 second-probe word
         asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
         // publication gate: a bounded poll, and no load in flight if it gives up
@@ -391,8 +429,12 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                 __nanosleep(1000);
             }
         }
-        if (open) issue(0);
-        else meta[3] = 0;
+        if (open) {
+            issue(0);
+        } else {
+            meta[3] = 0;
+            if constexpr (kStageBarriers) mbar_arrive(bar0);
+        }
     }
     __syncthreads();
 
@@ -452,30 +494,60 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
     uint32_t s2 = s1, s2_bmask = 0;
 
     for (uint32_t k = 0;; k++) {
-        const int* m = meta + 4 * (k & 1);
-        if (!m[3]) break;
-        const int job = m[0];
-        const uint32_t st = (uint32_t)m[1];
-        const int r = m[2];
-        if (tid == 0) issue(k + 1);
         const uint32_t bar = (k & 1) ? bar1 : bar0;
         const uint32_t parity = (k >> 1) & 1u;
-        uint32_t it = 0;
-        while (!mbar_try_wait(bar, parity)) {
-            if (++it >= kWaitLimit) {
-                atomicOr(error_flag, 4u);
-                s_abort = 1;
-                break;
-            }
-        }
-        if (s_abort) {
-            // Give the load issued for k + 1 a bounded chance to land before this CTA's shared memory goes away.
-            if (tid == 0 && meta[4 * ((k + 1) & 1) + 3]) {
-                const uint32_t nb = ((k + 1) & 1) ? bar1 : bar0;
-                for (uint32_t j = 0; j < kWaitLimit && !mbar_try_wait(nb, ((k + 1) >> 1) & 1u); j++) {
+        int job, r;
+        uint32_t st;
+        if constexpr (kStageBarriers) {
+            // Warps meet only through the stages' barriers: a warp may start stage k + 1 while others still
+            // read stage k, and thread 0 refills a stage once every warp has released it.
+            uint32_t it = 0;
+            while (!mbar_try_wait(bar, parity)) {
+                if (++it >= kWaitLimit) {
+                    atomicOr(error_flag, 4u);
+                    s_abort = 1;
+                    break;
                 }
             }
-            break;
+            if (s_abort) {
+                // Give a load still in flight a bounded chance to land before the shared memory goes away.
+                if (tid == 0 && meta[4 * (k & 1) + 3])
+                    for (uint32_t j = 0; j < kWaitLimit && !mbar_try_wait(bar, parity); j++) {
+                    }
+                break;
+            }
+            // the stage's meta is written before its full barrier completes, so it is read after the wait
+            const int* m = meta + 4 * (k & 1);
+            if (!m[3]) break;
+            job = m[0];
+            st = (uint32_t)m[1];
+            r = m[2];
+            if (tid == 0 && !issue(k + 1)) s_abort = 1;
+        } else {
+            // meta of stage k was written before the previous stage's block barrier
+            const int* m = meta + 4 * (k & 1);
+            if (!m[3]) break;
+            job = m[0];
+            st = (uint32_t)m[1];
+            r = m[2];
+            if (tid == 0) issue(k + 1);
+            uint32_t it = 0;
+            while (!mbar_try_wait(bar, parity)) {
+                if (++it >= kWaitLimit) {
+                    atomicOr(error_flag, 4u);
+                    s_abort = 1;
+                    break;
+                }
+            }
+            if (s_abort) {
+                // Give the load issued for k + 1 a bounded chance to land before the shared memory goes away.
+                if (tid == 0 && meta[4 * ((k + 1) & 1) + 3]) {
+                    const uint32_t nb = ((k + 1) & 1) ? bar1 : bar0;
+                    for (uint32_t j = 0; j < kWaitLimit && !mbar_try_wait(nb, ((k + 1) >> 1) & 1u); j++) {
+                    }
+                }
+                break;
+            }
         }
         if (job != cur_job) {
             cur_job = job;
@@ -499,6 +571,9 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
             s2 = two ? s1 : bar0 + 64;
             s2_bmask = two ? s1_bmask : 0u;
             if constexpr (kTable) {
+                // every warp is done with the previous job's table before it is overwritten (all warps change
+                // job at the same stage)
+                if constexpr (kStageBarriers) __syncthreads();
                 const uint32_t nw = s1_fits ? J->stage1_nwords : 0u;
                 const uint32_t* src = J->stage1_words;
                 for (uint32_t i = tid; i < nw; i += THREADS) s1p[i] = src[i];
@@ -509,7 +584,12 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
         // self-checks: a bad descriptor or sequencing records a code and skips the work
         if ((uint32_t)job >= n_jobs || st >= job_desc()->n_supertiles || r < -1 || r >= (int)R || !s1_fits) {
             if (tid == 0) atomicOr(error_flag, 0x100u);
-            __syncthreads();
+            if constexpr (kStageBarriers) {
+                __syncwarp();
+                if (lane == 0) mbar_arrive(ebar(k));
+            } else {
+                __syncthreads();
+            }
             continue;
         }
         const uint64_t z = (uint64_t)st * THREADS + tid;
@@ -643,7 +723,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                         return lds64(lane_tab + co * 128u);
                     };
                     uint2 nsv = make_uint2(0, 0), no = make_uint2(0, 0);
-                    if constexpr (MODE == 0) {
+                    if constexpr (kSparse) {
                         nsv = sbox_in(0);
                         no = sbox_out(0);
                     }
@@ -651,7 +731,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                     for (int j = 0; j < 32; j++) {
                         const uint32_t c = byte_at(cur[j >> 2], j & 3);
                         uint2 sv, o;
-                        if constexpr (MODE == 0) {
+                        if constexpr (kSparse) {
                             sv = nsv;
                             o = no;
                             if (j + 1 < 32) {
@@ -668,7 +748,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                         hl = nl ^ sv.x ^ rl;
                         hh = nh ^ sv.y ^ rh;
                         if (c == 0x0Au) lnp = j;
-                        if constexpr (MODE == 0) {
+                        if constexpr (kSparse) {
                             // with S = 1 the second probe reads a word of ones
                             const uint32_t w0 = lds32(s1 + ((hl >> 3) & s1_bmask));
                             const uint32_t w1 = lds32(s2 + ((hh >> 3) & s2_bmask));
@@ -712,7 +792,7 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                                 ring_v[slot] = ldg_if(main_words + (((fa & a_mask) + a_add) >> 5), issue);
                         }
                     }
-                    if constexpr (MODE == 0) {  // the block's last window
+                    if constexpr (kSparse) {  // the block's last window
                         const uint32_t t = __funnelshift_r(pw0, pw0, pl) & __funnelshift_r(pw1, pw1, ph);
                         enqueue(pv && (t & 1u) != 0, (uint32_t)(kRowBytes + 32 * b + 31), pl, ph, s1_first);
                     }
@@ -778,7 +858,13 @@ __global__ void __launch_bounds__(THREADS, ctas_per_sm(THREADS, MODE)) k_scan_fa
                 }
             }
         }
-        __syncthreads();
+        if constexpr (kStageBarriers) {
+            // this warp is done reading the stage
+            __syncwarp();
+            if (lane == 0) mbar_arrive(ebar(k));
+        } else {
+            __syncthreads();
+        }
     }
 }
 
@@ -800,14 +886,14 @@ constexpr size_t static_smem(int threads) { return 16 * (size_t)threads + 8 * (s
 template <int THREADS, int MODE>
 constexpr size_t fixed_smem() {
     return 1024 + 2 * (size_t)THREADS * kRowBytes + kTabBytes + 128 +
-           (THREADS / 32) * (size_t)(MODE == 0 || MODE == 4 ? kQueueBytes : 2 * kQueueBytes);
+           (THREADS / 32) * (size_t)(sparse_mode(MODE) || MODE == 4 ? kQueueBytes : 2 * kQueueBytes);
 }
 
 template <int L, int THREADS, int MODE>
 cudaError_t launch_cfg(const FastJob* d_jobs, uint32_t n_jobs, uint32_t n_items, uint32_t max_s1_words,
                        uint32_t* d_ctl, int num_sms, cudaStream_t st) {
     const size_t smem =
-        fixed_smem<THREADS, MODE>() + (MODE == 0 || MODE == 3 || MODE == 4 ? 4 * (size_t)max_s1_words : 0);
+        fixed_smem<THREADS, MODE>() + (sparse_mode(MODE) || MODE == 3 || MODE == 4 ? 4 * (size_t)max_s1_words : 0);
     cudaError_t e =
         cudaFuncSetAttribute(k_scan_fast<L, THREADS, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     if (e != cudaSuccess) return e;
@@ -836,6 +922,8 @@ cudaError_t launch_len(const FastConfig& cfg, const FastJob* d_jobs, uint32_t n_
         return cfg.threads == 256 ? launch_cfg<L, 256, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st)
                                   : launch_cfg<L, 384, 1>(d_jobs, n_jobs, n_items, 0, d_ctl, num_sms, st);
     }
+    if (cfg.mode == 3)  // sparse with per-stage barriers: 512 threads
+        return launch_cfg<L, 512, 5>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
     if (cfg.mode == 2) {  // sparse, deferred candidates: 192, 256 or 384 threads (larger stage-1 tables)
         switch (cfg.threads) {
             case 192: return launch_cfg<L, 192, 4>(d_jobs, n_jobs, n_items, max_s1_words, d_ctl, num_sms, st);
@@ -914,6 +1002,7 @@ int dense_probe_order(const Geom& g, double cache_fill, double ext_fill) {
 int config_threads(const FastConfig& cfg) {
     if (cfg.mode == 1) return cfg.threads == 256 ? 256 : cfg.threads == 192 && cfg.order != 2 ? 192 : 384;
     if (cfg.mode == 2) return cfg.threads == 192 || cfg.threads == 384 ? cfg.threads : 256;
+    if (cfg.mode == 3) return 512;
     return cfg.threads == 384 || cfg.threads == 512 ? cfg.threads : 256;
 }
 
@@ -971,7 +1060,7 @@ uint64_t fill_fast_job(const ScanArgs& a, const uint32_t* stage1_words, const Fa
     {
         // dense mode: regions of the pipelined probes, index functions f0/f1 (order 0) or f2/f3 (order 1,
         // which only K >= 4 filters set)
-        if (cfg.mode < 0 || cfg.mode > 2 ||
+        if (cfg.mode < 0 || cfg.mode > 3 ||
             (cfg.mode == 1 && (a.g.k < 2 || (cfg.order == 1 && a.g.k < 4) || cfg.order < 0 || cfg.order > 2)))
             *err = cudaErrorInvalidValue;
         const uint32_t fa = cfg.order == 1 ? 2u : 0u, fb = fa + 1;

@@ -371,7 +371,8 @@ class Filter:
 
     def config(self):
         """(threads, mode) of the tuned scan for this filter (mode 0: shared-memory stage, 1: L2 probes, 2:
-        shared-memory stage with candidates deferred to the end of each 32-byte block)."""
+        shared-memory stage with candidates deferred to the end of each 32-byte block, 3: mode 0 with
+        per-stage barriers instead of a block barrier per stage)."""
         t, m = ctypes.c_int(), ctypes.c_int()
         self._check(self._lib.ffbf_get_scan_config(self._h, ctypes.byref(t), ctypes.byref(m)))
         return t.value, m.value

@@ -267,7 +267,8 @@ ffbf_status ffbf_debug_scan_unpublished(ffbf_ctx* ctx, const uint8_t* d_text, si
 
 /* The tuned scan's current configuration for this context (CTA threads; mode 0 shared-memory stage 1 with
  * candidates queued per byte, 1 pipelined L2 probes, 2 shared-memory stage 1 with candidates deferred to the
- * end of each 32-byte block), as the autotuner or the filter's fill chose it. Before the first scan or tuning
+ * end of each 32-byte block, 3 mode 0 at 512 threads whose warps meet through per-stage barriers), as the
+ * autotuner or the filter's fill chose it. Before the first scan or tuning
  * it reports the defaults. */
 ffbf_status ffbf_get_scan_config(const ffbf_ctx* ctx, int* threads, int* mode);
 

@@ -145,7 +145,8 @@ public:
     ffbf_ctx* handle() { return ctx_; }
 
     // The tuned scan's configuration as the filter's fills or ffbf_autotune chose it: CTA threads, mode (0
-    // shared-memory stage, 1 pipelined L2 probes, 2 shared-memory stage with deferred candidates) and the
+    // shared-memory stage, 1 pipelined L2 probes, 2 shared-memory stage with deferred candidates, 3 shared-memory
+    // stage with per-stage barriers) and the
     // dense mode's probe order (0, 1 or 2).
     struct ScanConfig {
         int threads, mode, order;

@@ -179,6 +179,7 @@ SCAN_VARIANTS = [
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "256"},
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "384"},
     {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "512"},
+    {"FFBF_SCAN_MODE": "3"},
     {"FFBF_SCAN_MODE": "2", "FFBF_SCAN_THREADS": "192"},
     {"FFBF_SCAN_MODE": "2", "FFBF_SCAN_THREADS": "256"},
     {"FFBF_SCAN_MODE": "2", "FFBF_SCAN_THREADS": "384"},
@@ -198,8 +199,9 @@ SCAN_ENV = ("FFBF_FORCE_GENERIC_SCAN", "FFBF_SCAN_MODE", "FFBF_SCAN_THREADS", "F
 @pytest.mark.parametrize("name", ["plain_small", "scale_small", "smem_cache", "edge_chunks", "binary_small",
                                   "dense_fp", "len19_default"])
 def test_scan_variants_agree_with_oracle(name, monkeypatch):
-    """Every scan kernel variant (generic; tuned sparse at each CTA size, with candidates queued per byte or
-    deferred to the end of each 32-byte block; tuned dense in every probe order) is bit-exact."""
+    """Every scan kernel variant (generic; tuned sparse at each CTA size, with candidates queued per byte,
+    with per-stage barriers, or deferred to the end of each 32-byte block; tuned dense in every probe order)
+    is bit-exact."""
     prm, pats, text = build_inputs(name)
     o, s, _, _, _ = run_oracle(prm, pats, text)
     for env in SCAN_VARIANTS:
@@ -256,6 +258,7 @@ def test_dense_probe_orders_over_geometries(L, k, s, monkeypatch):
     pats, text = _gen(40 + k * 3 + s, dg.PRINTABLE, 3000, L, L + 16, 2_000_000, 80, 300)
     o, so, _, _, _ = run_oracle(prm, pats, text)
     variants = [{}, {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "384"}, {"FFBF_SCAN_MODE": "0", "FFBF_SCAN_THREADS": "512"},
+                {"FFBF_SCAN_MODE": "3"},
                 {"FFBF_SCAN_MODE": "2"}, {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "0"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1"},
                 {"FFBF_SCAN_MODE": "1", "FFBF_SCAN_ORDER": "1", "FFBF_SCAN_THREADS": "256"},
@@ -392,7 +395,7 @@ def test_cpp_mirror_program_matches_reference_files(tmp_path):
         assert g.matches("pruned", (tmp_path / "out").read_bytes())
         assert g.matches("index", (tmp_path / "__index_out").read_bytes())
         direct = int(re.search(rb"direct scan: (\d+) hits", r.stderr).group(1))
-        assert re.search(rb"scan config: (256|384|512) threads, mode [01], probe order [012]", r.stderr), r.stderr
+        assert re.search(rb"scan config: (192|256|384|512) threads, mode [0-3], probe order [012]", r.stderr), r.stderr
         if mode:
             served = int(re.search(rb"status 0, (\d+) hits", r.stderr).group(1))
             assert served == direct > 0
