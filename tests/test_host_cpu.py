@@ -117,6 +117,24 @@ def test_cpp_mirror_header_compiles_and_links(tmp_path):
     assert r.returncode == 1 and b"FilterError" in r.stderr
 
 
+def test_scan_sizing_rules_on_the_host(tmp_path):
+    """tests/cpp/row_model.cu, linked against libffbf.so, checks the tuned scan's rows per stream (waves of
+    items over the CTA slots, alone and in a batch), CTA sizes per configuration and the result sorts' key
+    widths; all host code, so it runs without a device."""
+    import shutil
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc):
+        pytest.skip("nvcc not available")
+    exe = str(tmp_path / "row_model")
+    lib = os.path.join(ROOT, "ffbf_b200", "_lib")
+    subprocess.run([nvcc, "-std=c++17", "-O2", f"-I{os.path.join(ROOT, 'include')}",
+                    f"-I{os.path.join(ROOT, 'ffbf_b200', 'csrc')}", os.path.join(ROOT, "tests", "cpp", "row_model.cu"),
+                    "-o", exe, f"-L{lib}", "-lffbf", f"-Xlinker=-rpath,{lib}", "-lcuda"], check=True,
+                   capture_output=True)
+    r = subprocess.run([exe], capture_output=True)
+    assert r.returncode == 0, r.stdout.decode() + r.stderr.decode()
+
+
 def _bench():
     import importlib.util
     spec = importlib.util.spec_from_file_location("bench_under_test", os.path.join(ROOT, "bench.py"))
